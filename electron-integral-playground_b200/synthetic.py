@@ -1,0 +1,170 @@
+"""Seeded synthetic molecules and basis sets for the benchmark workloads.
+
+No public benchmark suite exists for this path; these generators stand in for
+real chemistry with the shapes, sizes and value ranges the workloads name:
+
+* ``water_cluster(n_water, box_angstrom, seed)`` -- rigid waters (O-H 0.96 A,
+  H-O-H 104.5 deg), uniform random centres in a cube, uniform random
+  orientation (unit quaternion), O-O distance >= 2.6 A by rejection.
+* ``organic_molecule(n_atom, seed)`` -- H/C/N/O (0.5/0.3/0.1/0.1) grown by
+  random bonded placement: X-H 1.09 A, heavy-heavy U[1.40, 1.54] A, every
+  non-bonded distance >= 2.0 A.
+* ``orbital_basis_text(elements, seed)`` -- Gaussian-format text; O/C/N get
+  3s2p1d and H 2s1p.  Every shell draws 1-6 distinct exponents (uniform count)
+  from an even-tempered ladder of ratio 3.0 starting at 0.12 and capped at
+  5000 (heavy s) / 30 (H s), the cap shrinking by 10x per unit of angular
+  momentum; contraction coefficients are U[0.1, 1] before normalisation.
+* ``auxiliary_basis_text(elements, l_max)`` -- uncontracted even-tempered
+  shells, ratio 2.5 from 0.1 up to 200 (9 exponents per l), l = 0..l_max.
+
+All sizes in Angstrom on input; molecules are returned in Bohr like the XYZ
+reader does.
+"""
+
+import math
+
+import numpy as np
+
+from .basis_utility import ANGULAR_LETTERS, attach_auxiliary_basis_to_molecule, attach_basis_to_molecule
+from .data_structure import Molecule
+from .readers import angstrom_to_bohr, read_basis_content
+
+OH_ANGSTROM = 0.96
+HOH_DEGREES = 104.5
+
+
+def _random_rotation(rng):
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([
+        [1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+        [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+        [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)],
+    ])
+
+
+def water_cluster(n_water: int, box_angstrom: float, seed: int = 0, min_oo: float = 2.6) -> Molecule:
+    rng = np.random.default_rng(seed)
+    half = math.radians(HOH_DEGREES) / 2
+    local = np.array([[0.0, 0.0, 0.0],
+                      [OH_ANGSTROM * math.sin(half), 0.0, OH_ANGSTROM * math.cos(half)],
+                      [-OH_ANGSTROM * math.sin(half), 0.0, OH_ANGSTROM * math.cos(half)]])
+    centres = []
+    tries = 0
+    while len(centres) < n_water:
+        tries += 1
+        if tries > 1000000:
+            raise RuntimeError("could not place waters; box too small")
+        c = rng.uniform(0.0, box_angstrom, size=3)
+        if all(np.linalg.norm(c - o) >= min_oo for o in centres):
+            centres.append(c)
+    xyz, elements = [], []
+    for c in centres:
+        R = _random_rotation(rng)
+        for el, r in zip(("O", "H", "H"), local):
+            xyz.append(c + R @ r)
+            elements.append(el)
+    return Molecule(elements=elements, geometry=np.array(xyz) * angstrom_to_bohr, spherical_basis=True)
+
+
+def organic_molecule(n_atom: int, seed: int = 0) -> Molecule:
+    rng = np.random.default_rng(seed)
+    symbols = np.array(["H", "C", "N", "O"])
+    probs = np.array([0.5, 0.3, 0.1, 0.1])
+    heavy_probs = probs[1:] / probs[1:].sum()
+    elements = [str(rng.choice(symbols[1:], p=heavy_probs))]
+    xyz = [np.zeros(3)]
+    while len(elements) < n_atom:
+        el = str(rng.choice(symbols, p=probs))
+        heavy = [i for i, e in enumerate(elements) if e != "H"]
+        placed = False
+        for _ in range(200):
+            parent = heavy[rng.integers(len(heavy))]
+            bond = 1.09 if (el == "H") else rng.uniform(1.40, 1.54)
+            v = rng.normal(size=3)
+            pos = xyz[parent] + bond * v / np.linalg.norm(v)
+            ok = all(np.linalg.norm(pos - xyz[k]) >= 2.0 for k in range(len(xyz)) if k != parent)
+            if ok:
+                elements.append(el)
+                xyz.append(pos)
+                placed = True
+                break
+        if not placed:
+            # Crowded: fall back to a heavy atom so the skeleton can grow outwards.
+            continue
+    return Molecule(elements=elements, geometry=np.array(xyz) * angstrom_to_bohr, spherical_basis=True)
+
+
+_SHELLS = {"H": (2, 1, 0), "C": (3, 2, 1), "N": (3, 2, 1), "O": (3, 2, 1)}
+_S_CAP = {"H": 30.0, "C": 5000.0, "N": 5000.0, "O": 5000.0}
+
+
+def _ladder(start, ratio, cap):
+    out = []
+    e = start
+    while e <= cap * (1 + 1e-12):
+        out.append(e)
+        e *= ratio
+    return out
+
+
+def orbital_basis_text(elements, seed: int = 0) -> str:
+    rng = np.random.default_rng(seed + 7919)
+    lines = []
+    for el in sorted(set(elements)):
+        lines.append(f"{el}     0")
+        counts = _SHELLS[el]
+        for l, n_shell in enumerate(counts):
+            ladder = _ladder(0.12, 3.0, max(_S_CAP[el] / 10.0 ** l, 0.5))
+            for _ in range(n_shell):
+                k = int(rng.integers(1, 7))
+                k = min(k, len(ladder))
+                chosen = sorted(rng.choice(ladder, size=k, replace=False), reverse=True)
+                lines.append(f"{ANGULAR_LETTERS[l]}    {k}   1.00")
+                for e in chosen:
+                    lines.append(f"    {float(e)!r}    {float(rng.uniform(0.1, 1.0))!r}")
+        lines.append("****")
+    return "\n".join(lines) + "\n"
+
+
+def auxiliary_basis_text(elements, l_max: int) -> str:
+    ladder = _ladder(0.1, 2.5, 200.0)
+    lines = []
+    for el in sorted(set(elements)):
+        lines.append(f"{el}     0")
+        for l in range(l_max + 1):
+            for e in ladder:
+                lines.append(f"{ANGULAR_LETTERS[l]}    1   1.00")
+                lines.append(f"    {float(e)!r}    1.0")
+        lines.append("****")
+    return "\n".join(lines) + "\n"
+
+
+def attach_synthetic_basis(molecule: Molecule, aux_l_max: int, seed: int = 0, spherical: bool = True) -> Molecule:
+    molecule.spherical_basis = spherical
+    attach_basis_to_molecule(molecule, read_basis_content(orbital_basis_text(["H", "C", "N", "O"], seed)))
+    attach_auxiliary_basis_to_molecule(molecule, read_basis_content(auxiliary_basis_text(["H", "C", "N", "O"], aux_l_max)))
+    return molecule
+
+
+def config0_water10(seed: int = 0) -> Molecule:
+    """10 waters in a 9 A cube; aux s-f."""
+    return attach_synthetic_basis(water_cluster(10, 9.0, seed), aux_l_max=3, seed=seed)
+
+
+def config2_water100(seed: int = 0) -> Molecule:
+    """100 waters in a 15 A cube; aux s-f."""
+    return attach_synthetic_basis(water_cluster(100, 15.0, seed), aux_l_max=3, seed=seed)
+
+
+def molecule_sizes(n_molecule: int, lo: int, hi: int, seed: int):
+    rng = np.random.default_rng(seed + 104729)
+    return [int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))))) for _ in range(n_molecule)]
+
+
+def config1_batch(seed: int = 0, n_molecule: int = 64):
+    """64 organic molecules of 3-60 atoms (log-uniform); aux s-g."""
+    sizes = molecule_sizes(n_molecule, 3, 60, seed)
+    return [attach_synthetic_basis(organic_molecule(n, seed * 1000 + i), aux_l_max=4, seed=seed)
+            for i, n in enumerate(sizes)]
