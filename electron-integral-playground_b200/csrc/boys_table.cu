@@ -1,0 +1,67 @@
+// Device-resident constant tables: the Boys-function Taylor grid and run-time
+// copies of the spherical-harmonic / normalisation coefficients.
+#include <math.h>
+
+#include "eip_common.cuh"
+#include "eip_internal.h"
+
+namespace eip {
+
+__device__ double g_boys_table[kBoysGrid * kBoysOrders];
+static const double* g_boys_table_address = nullptr;
+
+const double* boys_table_device() { return g_boys_table_address; }
+
+// F_m(T0) on the grid: F_M(T0) = e^-T0 sum_k (2 T0)^k / ((2M+1)(2M+3)...(2M+2k+1))
+// (all terms positive: no cancellation), in long double, then the downward
+// recursion F_m = (2 T0 F_{m+1} + e^-T0) / (2m+1) for the lower orders.
+static void build_boys_table(double* out) {
+    const int M = kBoysOrders - 1;
+    for (int i = 0; i < kBoysGrid; i++) {
+        long double T = (long double)i * (long double)kBoysStep;
+        long double eT = expl(-T);
+        long double F[kBoysOrders];
+        long double term = 1.0L / (2 * M + 1), sum = term;
+        for (int k = 1; k < 10000; k++) {
+            term *= 2.0L * T / (2 * M + 2 * k + 1);
+            sum += term;
+            if (term < sum * 1e-22L) break;
+        }
+        F[M] = eT * sum;
+        for (int m = M - 1; m >= 0; m--) F[m] = (2.0L * T * F[m + 1] + eT) / (2 * m + 1);
+        for (int m = 0; m <= M; m++) out[i * kBoysOrders + m] = (double)F[m];
+    }
+}
+
+int upload_constant_tables() {
+    static double host_table[kBoysGrid * kBoysOrders];
+    static bool built = false;
+    if (!built) {
+        build_boys_table(host_table);
+        built = true;
+    }
+    cudaError_t e = cudaMemcpyToSymbol(g_boys_table, host_table, sizeof(host_table));
+    void* addr = nullptr;
+    if (e == cudaSuccess) e = cudaGetSymbolAddress(&addr, g_boys_table);
+    if (e != cudaSuccess) return (int)e;
+    g_boys_table_address = static_cast<const double*>(addr);
+    return upload_generic_tables();
+}
+
+// Evaluate F_0..F_L on the device for a list of T (tests the device Boys).
+__global__ void boys_probe_kernel(const double* __restrict__ table, int L, const double* T, int n, double* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double F[kMaxBoysM + 1];
+    boys_rt(table, L, T[i], F);
+    for (int m = 0; m <= L; m++) out[(size_t)i * (L + 1) + m] = F[m];
+}
+
+int launch_boys_probe(int L, const double* dT, int n, double* dout, cudaStream_t s) {
+    if (L < 0 || L > kMaxBoysM) return 1;
+    if (n <= 0) return 0;
+    boys_probe_kernel<<<(n + 127) / 128, 128, 0, s>>>(g_boys_table_address, L, dT, n, dout);
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+}  // namespace eip

@@ -1,0 +1,89 @@
+/*
+ * libmolecular_integral.so -- B200 (sm_100a) McMurchie-Davidson integrals.
+ *
+ * Drop-in C ABI.  The first four entry points are exactly the symbols the
+ * reference front end binds with ctypes.cdll.LoadLibrary("libmolecular_integral.so")
+ * (electron_integral_playground/molecular_integral/*.py:7) and have the same
+ * signatures, argument meaning, accumulate-into-output semantics, supported
+ * classes and error behaviour (return 0 on success; print a message and
+ * return 1 for an unsupported angular class).  Additionally they return 2 on
+ * a CUDA failure (no device, allocation or launch error); eip_last_error()
+ * then describes it.  All pointers are host pointers to C-contiguous arrays;
+ * positions in Bohr; (n,4) rows are [x, y, z, exponent].
+ *
+ * Layouts of the outputs (the caller zero-fills; the library adds):
+ *   three_center       J3c[n_aux][n_ao][n_ao]
+ *   two_center         J2c[n_aux][n_aux]
+ *   nuclear_attraction V[n_ao][n_ao][n_charge]   (not scaled by -Z)
+ *   overlap            S[n_ao][n_ao]
+ */
+#ifndef EIP_B200_H
+#define EIP_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces the reference three_center
+ * (electron_integral_playground/c_library/molecular_integral/three_center.cpp:321-340).
+ * One (l_i, l_j | l_k) class: i_L <= j_L <= 6, k_L <= 9. */
+int three_center(const int i_L, const int j_L, const int k_L,
+                 const double* pair_P_p, const double* pair_A_a, const double* pair_B_b,
+                 const double* pair_coefficient, const int* pair_i_ao_start, const int* pair_j_ao_start,
+                 const int n_pair_ij, const double* aux_A_a, const double* aux_coefficient,
+                 const int* aux_i_aux_start, const int n_aux_primitive_k, double* J3c_matrix,
+                 const int n_ao, const int n_aux, const bool spherical, const double omega);
+
+/* Replaces the reference two_center
+ * (electron_integral_playground/c_library/molecular_integral/two_center.cpp:239-252).
+ * i_L <= j_L <= 9; for i_L == j_L, primitive pairs with i_aux_start > j_aux_start
+ * are skipped and the other triangle is filled by mirroring, as in the reference. */
+int two_center(const int i_L, const int j_L,
+               const double* aux_A_a, const double* aux_i_coefficient, const int* aux_i_aux_start,
+               const int n_aux_primitive_i, const double* aux_B_b, const double* aux_j_coefficient,
+               const int* aux_j_aux_start, const int n_aux_primitive_j, double* J2c_matrix,
+               const int n_aux, const bool spherical, const double omega);
+
+/* Replaces the reference nuclear_attraction
+ * (electron_integral_playground/c_library/molecular_integral/nuclear_attraction.cpp:199-213).
+ * charge_position: (n_charge, 3) rows.  i_L <= j_L <= 6. */
+int nuclear_attraction(const int i_L, const int j_L,
+                       const double* pair_P_p, const double* pair_A_a, const double* pair_B_b,
+                       const double* pair_coefficient, const int* pair_i_ao_start,
+                       const int* pair_j_ao_start, const int n_pair, const double* charge_position,
+                       const int n_charge, double* V_tensor, const int n_ao, const bool spherical,
+                       const double omega);
+
+/* Replaces the reference overlap
+ * (electron_integral_playground/c_library/molecular_integral/overlap.cpp:149-159).  i_L <= j_L <= 6. */
+int overlap(const int i_L, const int j_L, const double* pair_A_a, const double* pair_B_b,
+            const double* pair_coefficient, const int* pair_i_ao_start, const int* pair_j_ao_start,
+            const int n_pair, double* S_matrix, const int n_ao, const bool spherical);
+
+/* ---- extensions (no counterpart in the reference) ------------------------ */
+
+/* Select the device (or -1: the current one) and create the library's stream
+ * and device tables.  Optional: every entry point initialises lazily. */
+int eip_init(int device);
+
+/* Description of the last CUDA failure of the calling thread ("" if none). */
+const char* eip_last_error(void);
+
+/* Number of kernels this process has launched through the library. */
+unsigned long long eip_kernel_launch_count(void);
+
+/* Device time (CUDA events on the library's stream) of the kernels of the
+ * last reference-ABI call, in milliseconds. */
+float eip_last_kernel_ms(void);
+
+/* Device Boys function: F[i*(L+1)+m] = F_m(T[i]), m = 0..L <= 21 (host buffers). */
+int eip_boys(int L, const double* T, int n, double* F);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EIP_B200_H */

@@ -1,0 +1,68 @@
+"""CPU-side checks of the C ABI library: it loads, exports every symbol the
+public header declares, and rejects unsupported classes before touching a
+device (no compute calls here)."""
+
+import ctypes
+import importlib
+import pathlib
+import re
+
+import numpy as np
+import pytest
+
+REPO = pathlib.Path(__file__).resolve().parent.parent
+lib_mod = importlib.import_module("electron-integral-playground_b200._lib")
+
+
+def declared_symbols():
+    text = (REPO / "include" / "eip_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(?:int|void|const char\s*\*|unsigned long long)\s+(\w+)\s*\(", text)))
+
+
+def test_header_declares_reference_abi():
+    syms = declared_symbols()
+    for s in ("three_center", "two_center", "nuclear_attraction", "overlap"):
+        assert s in syms
+
+
+def test_library_exports_declared_symbols():
+    if not lib_mod.LIB_PATH.exists():
+        pytest.skip("library not built")
+    L = ctypes.CDLL(str(lib_mod.LIB_PATH))
+    for s in declared_symbols():
+        assert hasattr(L, s), s
+
+
+def test_unsupported_class_rejected_without_device():
+    if not lib_mod.LIB_PATH.exists():
+        pytest.skip("library not built")
+    L = lib_mod.lib()
+    z = np.zeros(4)
+    zi = np.zeros(1, np.int32)
+    out = np.zeros(1)
+    dp, ip = lib_mod.dp, lib_mod.ip
+    assert L.three_center(7, 7, 0, dp(z), dp(z), dp(z), dp(z), ip(zi), ip(zi), 1, dp(z), dp(z), ip(zi), 1,
+                          dp(out), 1, 1, True, 0.0) == 1
+    assert L.three_center(2, 1, 0, dp(z), dp(z), dp(z), dp(z), ip(zi), ip(zi), 1, dp(z), dp(z), ip(zi), 1,
+                          dp(out), 1, 1, True, 0.0) == 1
+    assert L.three_center(0, 0, 10, dp(z), dp(z), dp(z), dp(z), ip(zi), ip(zi), 1, dp(z), dp(z), ip(zi), 1,
+                          dp(out), 1, 1, True, 0.0) == 1
+    assert L.two_center(3, 10, dp(z), dp(z), ip(zi), 1, dp(z), dp(z), ip(zi), 1, dp(out), 1, True, 0.0) == 1
+    assert L.nuclear_attraction(0, 7, dp(z), dp(z), dp(z), dp(z), ip(zi), ip(zi), 1, dp(z), 1, dp(out), 1, True,
+                                0.0) == 1
+    assert L.overlap(1, 0, dp(z), dp(z), dp(z), ip(zi), ip(zi), 1, dp(out), 1, True) == 1
+    assert out[0] == 0.0
+
+
+def test_empty_inputs_are_noops():
+    if not lib_mod.LIB_PATH.exists():
+        pytest.skip("library not built")
+    L = lib_mod.lib()
+    z = np.zeros(4)
+    zi = np.zeros(1, np.int32)
+    out = np.zeros(1)
+    dp, ip = lib_mod.dp, lib_mod.ip
+    assert L.three_center(0, 0, 0, dp(z), dp(z), dp(z), dp(z), ip(zi), ip(zi), 0, dp(z), dp(z), ip(zi), 1,
+                          dp(out), 1, 1, True, 0.0) == 0
+    assert L.overlap(0, 0, dp(z), dp(z), dp(z), ip(zi), ip(zi), 0, dp(out), 1, True) == 0

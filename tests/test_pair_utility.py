@@ -1,0 +1,60 @@
+"""The host pair builder against the reference front end: pair counts of the
+reference's own test (tests/test_pair_utility.py:24,46) and bit-identical
+pair tables for every golden case."""
+
+import importlib
+
+import numpy as np
+import pytest
+
+from golden_cases import GOLDEN, Case, case_names, _basis, _pairs
+
+pu = importlib.import_module("electron-integral-playground_b200.pair_utility")
+bu = importlib.import_module("electron-integral-playground_b200.basis_utility")
+ds = importlib.import_module("electron-integral-playground_b200.data_structure")
+
+REF_COUNTS = {
+    "pair_counts_compact": {(0, 0): 171, (0, 1): 158, (0, 2): 36, (1, 1): 51, (1, 2): 18, (2, 2): 3},
+    "pair_counts_sparse": {(0, 0): 144, (0, 1): 142, (0, 2): 34, (1, 1): 47, (1, 2): 18, (2, 2): 3},
+}
+
+
+def build(elements, geometry, basis, spherical=True):
+    mol = ds.Molecule(elements=list(elements), geometry=np.array(geometry), spherical_basis=spherical)
+    bu.attach_basis_to_molecule(mol, basis)
+    return mol
+
+
+@pytest.mark.parametrize("name", sorted(REF_COUNTS))
+def test_pair_counts(name):
+    d = np.load(GOLDEN / f"{name}.npz")
+    mol = build([str(x) for x in d["elements"]], d["geometry"], _basis(d, "basis__"))
+    lst = pu.form_primitive_pair_list(mol, 1e-14)
+    assert {k: len(v[0]) for k, v in lst.items()} == REF_COUNTS[name]
+    for k, v in lst.items():
+        bnd = v[4]
+        assert np.all(bnd[:-1] >= bnd[1:]) and np.all(bnd >= 1e-14)
+    mine = pu.form_pair_data(mol, 1e-14)
+    ref = _pairs(d, "pair__")
+    for k in ref:
+        for f in ("P_p", "A_a", "B_b", "coefficient", "i_ao_start", "j_ao_start"):
+            assert np.array_equal(getattr(mine[k], f), getattr(ref[k], f)), (k, f)
+
+
+@pytest.mark.parametrize("name", [n for n in case_names() if "two_center" not in n])
+def test_pair_tables_bit_identical(name):
+    c = Case(name)
+    mol = build(c.elements, c.geometry, c.basis, c.spherical)
+    assert mol.n_ao == c.n_ao
+    mine = pu.form_pair_data(mol, 1e-14)
+    assert list(mine) == list(c.pair_data) or set(mine) == set(c.pair_data)
+    for k, ref in c.pair_data.items():
+        for f in ("P_p", "A_a", "B_b", "coefficient", "i_ao_start", "j_ao_start"):
+            assert np.array_equal(getattr(mine[k], f), getattr(ref, f)), (k, f)
+    if c.aux_basis is not None:
+        bu.attach_auxiliary_basis_to_molecule(mol, c.aux_basis)
+        assert mol.n_aux == c.n_aux
+        aux = pu.form_auxiliary_pair_data(mol)
+        for k, ref in c.aux_data.items():
+            for f in ("A_a", "coefficient", "i_ao_start"):
+                assert np.array_equal(getattr(aux[k], f), getattr(ref, f)), (k, f)
