@@ -1,0 +1,323 @@
+#!/usr/bin/env python
+"""Benchmark: screened (mu nu|P) triplets/s on the batched B200 path.
+
+Workload (one "step"): every (mu nu|P) integral of 64 seeded synthetic organic
+molecules of 3-60 atoms (log-uniform; H/C/N/O 0.5/0.3/0.1/0.1; bonded growth;
+orbital 3s2p1d / H 2s1p contracted, auxiliary uncontracted s-g), computed as
+one CUDA-graph launch of the batched library path into a packed device
+buffer.  Metric unit: contracted shell triplets with Schwarz-type bound
+>= 1e-14 per second (all of them are computed).
+
+  value   device-resident tables, K graph launches timed with CUDA events on
+          the library's stream;
+  e2e     through the C ABI each step: H2D copy of every input table from the
+          batch's pinned host copy, the graph, and a D2H read of the step's
+          result (one checksum per molecule, accumulated in the kernels'
+          epilogue);
+  roofline  the class kernel with the largest device time, run alone,
+          algorithmic FLOPs (roofline.py) / its CUDA-event time, against the
+          FP64 FMA peak measured on the same GPU by the library's
+          microbenchmark;
+  cpu_baseline  the reference library (oracle/_ref, its own C++/OpenMP path)
+          on a bounded sample of the same molecules, all host cores.
+
+`--impl reference` times only that reference path (per step: the sample) and
+prints its own line.  Under torchrun each rank runs its own 64 molecules
+(seed + rank): independent shards, no data-path collective (weak scaling).
+"""
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "screened (μν|P) triplets/s, mixed vs FP64 at ≤1e-10 abs; p50/p99 latency"
+UNIT = "triplets/s"
+WORKLOAD = ("config-1 batched uneven sizes: 64 organic molecules of 3-60 atoms (log-uniform, H/C/N/O), "
+            "orbital 3s2p1d/2s1p contracted, auxiliary s-g uncontracted, all (mu nu|P) spherical, "
+            "one CUDA-graph launch")
+THRESHOLD = 1e-14
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def build_workload(seed, n_mol):
+    import importlib
+
+    syn = importlib.import_module("electron-integral-playground_b200.synthetic")
+    pu = importlib.import_module("electron-integral-playground_b200.pair_utility")
+    rf = importlib.import_module("electron-integral-playground_b200.roofline")
+    mols = syn.config1_batch(seed, n_mol)
+    pds = [pu.form_pair_data(m, 1e-14) for m in mols]
+    ads = [pu.form_auxiliary_pair_data(m) for m in mols]
+    stats = [rf.class_statistics(pd, ad, THRESHOLD) for pd, ad in zip(pds, ads)]
+    return mols, pds, ads, stats
+
+
+def reference_sample(mols, pds, ads, stats, budget_s, max_dense=2.0e8):
+    """Time the reference library on molecules (in batch order, skipping any whose
+    dense output exceeds max_dense doubles) until budget_s seconds elapse."""
+    import numpy as np
+    import oracle
+
+    ref = oracle.reference()
+    if ref is None:
+        return None
+    done, triplets, t_total = [], 0, 0.0
+    for i, m in enumerate(mols):
+        if m.n_aux * m.n_ao * m.n_ao > max_dense:
+            continue
+        t0 = time.perf_counter()
+        oracle.drive_three_center(ref, pds[i], ads[i], m)
+        t_total += time.perf_counter() - t0
+        triplets += sum(d["screened"] for d in stats[i].values())
+        done.append(i)
+        if t_total >= budget_s:
+            break
+    return dict(value=triplets / t_total, seconds=t_total, molecules=done, triplets=triplets,
+                cores=os.cpu_count())
+
+
+class ClockSampler:
+    def __init__(self, path):
+        self.path = path
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+            self.f.close()
+
+    def summary(self, device_index):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
+        except Exception:
+            return None
+        rows = [[x.strip() for x in r] for r in rows if len(r) >= 9 and r[0].strip() == str(device_index)]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        for r in rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]),
+                "reasons": sorted(reasons), "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows)}
+
+
+def run_reference_arm(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    mols, pds, ads, stats = build_workload(args.seed, args.molecules)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        s = reference_sample(mols, pds, ads, stats, args.ref_budget)
+        if s is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference library not built (make -C oracle ref)"}))
+            return
+        if i >= args.warmup:
+            vals.append(s)
+    v = statistics.mean(x["value"] for x in vals)
+    ms = statistics.mean(x["seconds"] for x in vals) * 1e3
+    sample = (f"molecules {vals[0]['molecules']} of the batch (dense output <= 2e8 doubles each), "
+              f"{vals[0]['triplets']} screened triplets per step")
+    print(json.dumps({
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generators; no dataset)", "impl": "reference",
+        "config": {"workload": WORKLOAD, "molecules": args.molecules, "seed": args.seed},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": vals[0]["cores"], "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--molecules", type=int, default=64)
+    ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of reference CPU work per sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import importlib
+
+    bt = importlib.import_module("electron-integral-playground_b200.batch")
+    rf = importlib.import_module("electron-integral-playground_b200.roofline")
+    lm = importlib.import_module("electron-integral-playground_b200._lib")
+    if lm.lib().eip_init(local) != 0:
+        raise RuntimeError(lm.lib().eip_last_error().decode())
+
+    mols, pds, ads, stats = build_workload(args.seed + 1000 * rank, args.molecules)
+    tot, per_class = rf.totals(stats)
+    batch = bt.ThreeCenterBatch(mols, pds, ads)
+    free, total_mem = torch.cuda.mem_get_info()
+    if batch.output_bytes > free - (2 << 30):
+        raise RuntimeError(f"packed output {batch.output_bytes / 1e9:.1f} GB exceeds free device memory")
+    batch.alloc_output()
+    stream = torch.cuda.ExternalStream(batch.stream)
+
+    def timed(fn, k):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        per = []
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ev0.record(stream)
+        marks = []
+        for _ in range(k):
+            e = torch.cuda.Event(enable_timing=True)
+            fn()
+            e.record(stream)
+            marks.append(e)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        last = ev0
+        for e in marks:
+            per.append(last.elapsed_time(e))
+            last = e
+        total = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([total], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            total = float(t.item())
+        return total, per
+
+    for _ in range(args.warmup):
+        batch.run(sync=False)
+    torch.cuda.synchronize()
+    clocks_path = str(REPO / "gpurun_out" / f"clocks_rank{rank}.csv") if (REPO / "gpurun_out").is_dir() else \
+        f"/tmp/eip_clocks_{os.getpid()}.csv"
+    with ClockSampler(clocks_path) as cs:
+        total_ms, per_step = timed(lambda: batch.run(sync=False), args.steps)
+    clocks = cs.summary(local)
+
+    # e2e: H2D of every input table + graph + D2H of the per-molecule checksums.
+    h_ck = np.empty(len(mols))
+
+    def e2e_step():
+        batch.upload()
+        batch.run(checksum=True, sync=False)
+        batch._check(batch.L.eip_batch_checksums(batch.h, lm.dp(h_ck)), "checksums")
+
+    for _ in range(2):
+        e2e_step()
+    t0 = time.perf_counter()
+    e2e_ms, _ = timed(e2e_step, args.steps)
+    e2e_wall_ms = (time.perf_counter() - t0) * 1e3
+
+    # Per-class device time (each class kernel alone, 2 launches, CUDA events).
+    class_ms = {}
+    for (li, lj, lk) in sorted(per_class):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if not batch.run_class(li, lj, lk):
+            continue
+        ev0.record(stream)
+        for _ in range(2):
+            batch.run_class(li, lj, lk)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        class_ms[(li, lj, lk)] = ev0.elapsed_time(ev1) / 2
+    fp64_peak = bt.measure_fma_peak(True)
+
+    screened = tot["screened"] * world
+    ms_step = total_ms / args.steps
+    value = screened / (ms_step * 1e-3)
+    dom = max(class_ms, key=class_ms.get) if class_ms else None
+    roof = None
+    if dom:
+        achieved = per_class[dom]["flops"] / (class_ms[dom] * 1e-3) / 1e12
+        traffic = None
+        tfile = REPO / "profiles" / "k3c_fast_traffic.txt"
+        if tfile.exists():
+            for line in tfile.read_text().splitlines():
+                if line.startswith(f"dram_bytes_per_launch {dom[0]}{dom[1]}{dom[2]} "):
+                    traffic = float(line.split()[2])
+        roof = {"bound": "fp64", "kernel": f"k3c_fast<{dom[0]},{dom[1]},{dom[2]}>", "achieved": achieved,
+                "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic,
+                "peak_source": "FP64 FMA microbenchmark on this GPU (eip_measure_fma_peak), this run",
+                "algorithmic_flops_per_launch": per_class[dom]["flops"], "ms_per_launch": class_ms[dom],
+                "whole_step_tflops": tot["flops"] / (ms_step * 1e-3) / 1e12,
+                "whole_step_frac": tot["flops"] / (ms_step * 1e-3) / 1e12 / fp64_peak,
+                "output_store_gbs": tot["out_bytes"] / (ms_step * 1e-3) / 1e9}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        s = reference_sample(mols, pds, ads, stats, args.ref_budget)
+        if s is not None:
+            cpu = {"value": s["value"], "unit": UNIT, "cores": s["cores"], "kind": "reference",
+                   "sample": f"molecules {s['molecules']} of the batch (dense output <= 2e8 doubles each), "
+                             f"{s['triplets']} screened triplets, {s['seconds']:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators; no dataset)",
+            "config": {"workload": WORKLOAD, "molecules": args.molecules * world, "seed": args.seed,
+                       "atoms": sum(len(m.elements) for m in mols) * world, "precision": "fp64",
+                       "classes": len(per_class), "primitive_triplets_per_step": tot["primitive"] * world,
+                       "contracted_triplets_per_step": tot["contracted"] * world,
+                       "screened_triplets_per_step": screened, "threshold": THRESHOLD,
+                       "packed_output_bytes": batch.output_bytes, "input_table_bytes": batch.table_bytes,
+                       "l2": "inputs + packed output per step exceed the 126 MB L2 (no flush needed)",
+                       "parallelism": f"{world} independent shard(s)"},
+            "e2e": {"value": screened / (e2e_ms / args.steps * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": batch.table_bytes, "d2h_bytes_per_step": 8 * len(mols),
+                    "wall_ms_per_step": e2e_wall_ms / args.steps,
+                    "result": "per-molecule checksum of the packed (mu nu|P) (computed in the kernels' epilogue)"},
+            "roofline": roof, "cpu_baseline": cpu,
+            "gpu_launches": batch.launches_per_run * args.steps, "clocks": clocks,
+            "latency_ms": {"p50": statistics.median(per_step),
+                           "p99": sorted(per_step)[min(len(per_step) - 1, int(0.99 * len(per_step)))]},
+            "class_ms": {f"{k[0]}{k[1]}|{k[2]}": round(v, 4) for k, v in sorted(class_ms.items())},
+        }
+        print(json.dumps(line))
+    batch.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

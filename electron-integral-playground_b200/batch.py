@@ -1,0 +1,205 @@
+"""Batched (mu nu|P) over many molecules (the eip_batch_* C ABI).
+
+All molecules' pair and auxiliary tables are uploaded once and stay on the
+device; every run is one CUDA-graph launch that computes every
+(l_i, l_j | l_k) class of every molecule into a packed device buffer
+(one block per molecule and class, layout [pair shell][I][J][K][aux shell]).
+``dense(m)`` expands molecule m's blocks into the reference's dense
+(n_aux, n_ao, n_ao) layout (used by tests; the packed form is the product).
+"""
+
+import ctypes
+
+import numpy as np
+
+from ._lib import IntegralError, as_f64, as_i32, dp, ip, lib
+
+_vp = ctypes.c_void_p
+
+
+def _bind(L):
+    if getattr(L, "_batch_bound", False):
+        return
+    c_int, c_double, c_bool, c_ll = ctypes.c_int, ctypes.c_double, ctypes.c_bool, ctypes.c_longlong
+    _dpp = ctypes.POINTER(ctypes.c_double)
+    _ipp = ctypes.POINTER(ctypes.c_int)
+    L.eip_batch_create.argtypes = [c_int, c_bool, c_double]
+    L.eip_batch_create.restype = _vp
+    L.eip_batch_add_pairs.argtypes = [_vp, c_int, c_int, c_int, _dpp, _dpp, _dpp, _dpp, _ipp, _ipp, c_int]
+    L.eip_batch_add_aux.argtypes = [_vp, c_int, c_int, _dpp, _dpp, _ipp, c_int]
+    L.eip_batch_build.argtypes = [_vp]
+    L.eip_batch_output_elems.argtypes = [_vp]
+    L.eip_batch_output_elems.restype = c_ll
+    L.eip_batch_block.argtypes = [_vp, c_int, c_int, c_int, c_int, ctypes.POINTER(c_ll), _ipp, _ipp]
+    L.eip_batch_alloc_output.argtypes = [_vp]
+    L.eip_batch_bind_output.argtypes = [_vp, _vp]
+    L.eip_batch_output_device.argtypes = [_vp]
+    L.eip_batch_output_device.restype = _vp
+    L.eip_batch_run.argtypes = [_vp, c_int]
+    L.eip_batch_run_class.argtypes = [_vp, c_int, c_int, c_int]
+    L.eip_batch_sync.argtypes = [_vp]
+    L.eip_batch_status.argtypes = [_vp]
+    L.eip_batch_upload.argtypes = [_vp]
+    L.eip_batch_table_bytes.argtypes = [_vp]
+    L.eip_batch_table_bytes.restype = c_ll
+    L.eip_batch_launches_per_run.argtypes = [_vp]
+    L.eip_batch_launches_per_run.restype = ctypes.c_ulonglong
+    L.eip_batch_checksums.argtypes = [_vp, _dpp]
+    L.eip_batch_copy_output.argtypes = [_vp, c_ll, c_ll, _dpp]
+    L.eip_batch_stream.argtypes = [_vp]
+    L.eip_batch_stream.restype = _vp
+    L.eip_batch_error.argtypes = [_vp]
+    L.eip_batch_error.restype = ctypes.c_char_p
+    L.eip_batch_destroy.argtypes = [_vp]
+    L.eip_batch_destroy.restype = None
+    L._batch_bound = True
+
+
+class ThreeCenterBatch:
+    def __init__(self, molecules, pair_data_list, aux_data_list, omega: float = 0.0):
+        if not (len(molecules) == len(pair_data_list) == len(aux_data_list)) or not molecules:
+            raise ValueError("need one pair table and one auxiliary table per molecule")
+        spherical = {bool(m.spherical_basis) for m in molecules}
+        if len(spherical) != 1:
+            raise ValueError("all molecules of a batch must share spherical_basis")
+        self.L = lib()
+        _bind(self.L)
+        self.molecules = molecules
+        self.pair_data_list = pair_data_list
+        self.aux_data_list = aux_data_list
+        self.spherical = spherical.pop()
+        self.omega = float(omega)
+        self.h = self.L.eip_batch_create(len(molecules), self.spherical, self.omega)
+        if not self.h:
+            raise IntegralError("eip_batch_create failed")
+        self._keep = []
+        for m, (pd, ad) in enumerate(zip(pair_data_list, aux_data_list)):
+            for (li, lj), p in pd.items():
+                arrs = [as_f64(p.P_p, (4,)), as_f64(p.A_a, (4,)), as_f64(p.B_b, (4,)), as_f64(p.coefficient),
+                        as_i32(p.i_ao_start), as_i32(p.j_ao_start)]
+                self._keep.append(arrs)
+                self._check(self.L.eip_batch_add_pairs(self.h, m, int(li), int(lj), dp(arrs[0]), dp(arrs[1]),
+                                                       dp(arrs[2]), dp(arrs[3]), ip(arrs[4]), ip(arrs[5]),
+                                                       arrs[0].shape[0]), "add_pairs")
+            for lk, a in ad.items():
+                arrs = [as_f64(a.A_a, (4,)), as_f64(a.coefficient), as_i32(a.i_ao_start)]
+                self._keep.append(arrs)
+                self._check(self.L.eip_batch_add_aux(self.h, m, int(lk), dp(arrs[0]), dp(arrs[1]), ip(arrs[2]),
+                                                     arrs[0].shape[0]), "add_aux")
+        self._check(self.L.eip_batch_build(self.h), "build")
+        self._keep = None
+        self.output_elems = int(self.L.eip_batch_output_elems(self.h))
+
+    def _check(self, rc, what):
+        if rc == 1:
+            raise IntegralError(f"eip_batch_{what}: unsupported angular class")
+        if rc != 0:
+            raise IntegralError(f"eip_batch_{what}: {self.L.eip_batch_error(self.h).decode(errors='replace')}")
+
+    @property
+    def output_bytes(self):
+        return 8 * self.output_elems
+
+    def alloc_output(self):
+        self._check(self.L.eip_batch_alloc_output(self.h), "alloc_output")
+
+    def bind_output(self, device_ptr: int):
+        self._check(self.L.eip_batch_bind_output(self.h, ctypes.c_void_p(device_ptr)), "bind_output")
+
+    def run(self, checksum: bool = False, sync: bool = True):
+        self._check(self.L.eip_batch_run(self.h, 1 if checksum else 0), "run")
+        if sync:
+            self.sync()
+
+    def run_class(self, li, lj, lk):
+        """Launch one class's kernel alone on the batch stream (per-kernel timing)."""
+        rc = self.L.eip_batch_run_class(self.h, li, lj, lk)
+        if rc == 1:
+            return False
+        self._check(rc, "run_class")
+        return True
+
+    def sync(self):
+        self._check(self.L.eip_batch_sync(self.h), "sync")
+
+    def status(self):
+        """Raise if a class kernel of the last run recorded a failed self-check."""
+        rc = self.L.eip_batch_status(self.h)
+        if rc != 0:
+            raise IntegralError(f"eip_batch_status: {self.L.eip_batch_error(self.h).decode(errors='replace')}")
+
+    def upload(self):
+        self._check(self.L.eip_batch_upload(self.h), "upload")
+
+    @property
+    def table_bytes(self):
+        return int(self.L.eip_batch_table_bytes(self.h))
+
+    @property
+    def launches_per_run(self):
+        return int(self.L.eip_batch_launches_per_run(self.h))
+
+    @property
+    def stream(self):
+        return self.L.eip_batch_stream(self.h)
+
+    def checksums(self):
+        out = np.empty(len(self.molecules))
+        self._check(self.L.eip_batch_checksums(self.h, dp(out)), "checksums")
+        return out
+
+    def block(self, m, li, lj, lk):
+        off, nsp, nax = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int()
+        rc = self.L.eip_batch_block(self.h, m, li, lj, lk, ctypes.byref(off), ctypes.byref(nsp), ctypes.byref(nax))
+        if rc != 0:
+            return None
+        return off.value, nsp.value, nax.value
+
+    def dense(self, m):
+        """Molecule m's (mu nu|P) in the reference's dense layout (n_aux, n_ao, n_ao)."""
+        mol = self.molecules[m]
+        J = np.zeros((mol.n_aux, mol.n_ao, mol.n_ao))
+        sph = self.spherical
+        n_of = (lambda l: 2 * l + 1) if sph else (lambda l: (l + 1) * (l + 2) // 2)
+        for (li, lj), p in self.pair_data_list[m].items():
+            pairs = np.unique(np.stack([np.asarray(p.i_ao_start), np.asarray(p.j_ao_start)], 1), axis=0)
+            for lk, a in self.aux_data_list[m].items():
+                blk = self.block(m, li, lj, lk)
+                if blk is None or blk[1] == 0 or blk[2] == 0:
+                    continue
+                off, nsp, nax = blk
+                ni, nj, nk = n_of(li), n_of(lj), n_of(lk)
+                buf = np.empty(nsp * ni * nj * nk * nax)
+                self._check(self.L.eip_batch_copy_output(self.h, off, buf.size, dp(buf)), "copy_output")
+                buf = buf.reshape(nsp, ni, nj, nk, nax)
+                aux0 = np.unique(np.asarray(a.i_ao_start))
+                assert pairs.shape[0] == nsp and aux0.shape[0] == nax
+                I = pairs[:, 0][:, None, None, None, None] + np.arange(ni)[None, :, None, None, None]
+                Jc = pairs[:, 1][:, None, None, None, None] + np.arange(nj)[None, None, :, None, None]
+                K = aux0[None, None, None, None, :] + np.arange(nk)[None, None, None, :, None]
+                I, Jc, K = np.broadcast_arrays(I, Jc, K)
+                J[K, I, Jc] = buf
+                off_diag = np.broadcast_to((pairs[:, 0] != pairs[:, 1])[:, None, None, None, None], buf.shape)
+                J[K[off_diag], Jc[off_diag], I[off_diag]] = buf[off_diag]
+        return J
+
+    def close(self):
+        if self.h:
+            self.L.eip_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def measure_fma_peak(fp64: bool = True) -> float:
+    """FP64 (or FP32) FMA throughput of the current device in TFLOP/s."""
+    L = lib()
+    L.eip_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    v = ctypes.c_double()
+    if L.eip_measure_fma_peak(1 if fp64 else 0, ctypes.byref(v)) != 0:
+        raise IntegralError("FMA peak microbenchmark failed")
+    return v.value

@@ -1,0 +1,595 @@
+// Batched (mu nu|P) over many molecules: the eip_batch_* C ABI.
+//
+// A batch holds the pair and auxiliary tables of many molecules (the same
+// structure-of-arrays format the reference ABI takes, one call per molecule
+// and class), builds device-resident tables once (primitive pairs grouped by
+// contracted shell pair, auxiliary primitives by shell, all molecules of one
+// class concatenated), and captures ONE CUDA graph per batch that runs:
+//   zero the work counters and checksums -> E-table kernels of every pair
+//   class -> every (l_i, l_j | l_k) class kernel over all molecules at once
+//   (persistent, atomic work list), forked over several streams so classes
+//   overlap.
+// Classes outside the fast kernels' range run as generic raw + transform
+// kernels, one pair per molecule, inside the same graph.
+// Output: one packed block per (molecule, class), offsets from
+// eip_batch_block(); see k3c_fast.cuh for the layout.
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <numeric>
+#include <vector>
+
+#include "eip_common.cuh"
+#include "eip_internal.h"
+#include "../../include/eip_b200.h"
+
+namespace eip {
+namespace {
+
+struct PairIn {
+    std::vector<double> P, A, B, coef;
+    std::vector<int> ia, ja;
+};
+struct AuxIn {
+    std::vector<double> C, coef;
+    std::vector<int> start;
+};
+
+struct ClassPlan {
+    int li, lj, lk;
+    bool fast;
+    int total_items = 0;
+    BraTable bra{};
+    KetTable ket{};
+    BatchMap map{};
+    int* counter = nullptr;
+    std::vector<long long> out_begin;   // per molecule
+    std::vector<int> n_sp, n_auxsh;     // per molecule
+    std::vector<int> sp0, aux0;         // per molecule (global indices in class tables)
+    long long out_elems = 0;
+    double flops_weight = 0;            // for scheduling order
+};
+
+template <typename T>
+T* at(void* base, size_t off) {
+    return reinterpret_cast<T*>(static_cast<char*>(base) + off);
+}
+
+struct Layout {
+    size_t total = 0;
+    size_t add(size_t bytes) {
+        size_t off = total;
+        total += (bytes + 255) & ~size_t(255);
+        return off;
+    }
+};
+
+}  // namespace
+}  // namespace eip
+
+using namespace eip;
+
+struct eip_batch {
+    int n_mol = 0;
+    bool spherical = true;
+    double omega = 0.0;
+    std::vector<std::map<std::pair<int, int>, PairIn>> pairs;  // per molecule
+    std::vector<std::map<int, AuxIn>> aux;                     // per molecule
+    bool built = false;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> events;
+    void* h_tables = nullptr;  // pinned copy of every device table (uploaded by eip_batch_upload)
+    void* d_tables = nullptr;
+    size_t table_bytes = 0;
+    double* d_etab = nullptr;
+    double* d_scratch = nullptr;
+    size_t scratch_elems = 0;
+    double* d_out = nullptr;
+    bool own_out = false;
+    double* d_checksum = nullptr;
+    long long out_elems = 0;
+    std::vector<ClassPlan> plans;
+    std::map<std::pair<int, int>, BraTable> bra_by_class;
+    std::map<std::pair<int, int>, size_t> etab_offset;
+    std::map<std::pair<int, int>, std::vector<int>> bra_sp_begin;  // per molecule prefix
+    std::map<int, std::vector<int>> ket_aux_begin;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches_per_run = 0;
+    char err[256] = "";
+};
+
+namespace {
+
+int fail(eip_batch* b, const char* what, cudaError_t e) {
+    snprintf(b->err, sizeof b->err, "%s: %s", what, e == cudaSuccess ? "invalid" : cudaGetErrorString(e));
+    fprintf(stderr, "[eip batch] %s\n", b->err);
+    return 2;
+}
+
+void group_indices(const int* ia, const int* ja, int n, std::vector<int>& order, std::vector<int>& begin,
+                   std::vector<int>& gi, std::vector<int>& gj) {
+    order.resize(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const int jx = ja ? ja[x] : 0, jy = ja ? ja[y] : 0;
+        return ia[x] != ia[y] ? ia[x] < ia[y] : jx < jy;
+    });
+    begin.clear();
+    gi.clear();
+    gj.clear();
+    for (int k = 0; k < n; k++) {
+        const int p = order[k];
+        const int jp = ja ? ja[p] : 0;
+        if (k == 0 || ia[p] != gi.back() || jp != gj.back()) {
+            begin.push_back(k);
+            gi.push_back(ia[p]);
+            gj.push_back(jp);
+        }
+    }
+    begin.push_back(n);
+}
+
+}  // namespace
+
+extern "C" {
+
+eip_batch* eip_batch_create(int n_molecules, bool spherical, double omega) {
+    if (n_molecules <= 0 || omega < 0.0) return nullptr;
+    eip_batch* b = new eip_batch;
+    b->n_mol = n_molecules;
+    b->spherical = spherical;
+    b->omega = omega;
+    b->pairs.resize(n_molecules);
+    b->aux.resize(n_molecules);
+    return b;
+}
+
+const char* eip_batch_error(eip_batch* b) { return b ? b->err : "null batch"; }
+
+int eip_batch_add_pairs(eip_batch* b, int mol, int i_L, int j_L, const double* P_p, const double* A_a,
+                        const double* B_b, const double* coefficient, const int* i_ao_start, const int* j_ao_start,
+                        int n_pair) {
+    if (!b || b->built || mol < 0 || mol >= b->n_mol || n_pair < 0) return 2;
+    if (i_L < 0 || i_L > j_L || j_L > kMaxOrbitalL) return 1;
+    PairIn& p = b->pairs[mol][{i_L, j_L}];
+    p.P.insert(p.P.end(), P_p, P_p + 4 * (size_t)n_pair);
+    p.A.insert(p.A.end(), A_a, A_a + 4 * (size_t)n_pair);
+    p.B.insert(p.B.end(), B_b, B_b + 4 * (size_t)n_pair);
+    p.coef.insert(p.coef.end(), coefficient, coefficient + n_pair);
+    p.ia.insert(p.ia.end(), i_ao_start, i_ao_start + n_pair);
+    p.ja.insert(p.ja.end(), j_ao_start, j_ao_start + n_pair);
+    return 0;
+}
+
+int eip_batch_add_aux(eip_batch* b, int mol, int k_L, const double* A_a, const double* coefficient,
+                      const int* aux_start, int n_primitive) {
+    if (!b || b->built || mol < 0 || mol >= b->n_mol || n_primitive < 0) return 2;
+    if (k_L < 0 || k_L > kMaxAuxL) return 1;
+    AuxIn& a = b->aux[mol][k_L];
+    a.C.insert(a.C.end(), A_a, A_a + 4 * (size_t)n_primitive);
+    a.coef.insert(a.coef.end(), coefficient, coefficient + n_primitive);
+    a.start.insert(a.start.end(), aux_start, aux_start + n_primitive);
+    return 0;
+}
+
+int eip_batch_build(eip_batch* b) {
+    if (!b || b->built) return 2;
+    if (int rc = eip_init(-1)) return fail(b, eip_last_error(), cudaSuccess) ? rc : rc;
+    cudaError_t e;
+    // ---- which classes exist
+    std::map<std::pair<int, int>, int> pair_classes;
+    std::map<int, int> aux_classes;
+    for (int m = 0; m < b->n_mol; m++) {
+        for (auto& kv : b->pairs[m]) pair_classes[kv.first] = 1;
+        for (auto& kv : b->aux[m]) aux_classes[kv.first] = 1;
+    }
+    // ---- group and lay out every table
+    struct BraHost {
+        std::vector<int> begin;
+        std::vector<int2> ao;
+        std::vector<double4> AB, P, PA;
+        std::vector<int> sp_begin;  // per molecule prefix (n_mol + 1)
+    };
+    struct KetHost {
+        std::vector<int> begin, start;
+        std::vector<double4> C;
+        std::vector<double> coef;
+        std::vector<int> aux_begin;
+    };
+    std::map<std::pair<int, int>, BraHost> bh;
+    std::map<int, KetHost> kh;
+    std::vector<int> order, gb, gi, gj;
+    for (auto& pc : pair_classes) {
+        BraHost& H = bh[pc.first];
+        H.begin.push_back(0);
+        H.sp_begin.push_back(0);
+        for (int m = 0; m < b->n_mol; m++) {
+            auto it = b->pairs[m].find(pc.first);
+            if (it != b->pairs[m].end() && !it->second.ia.empty()) {
+                const PairIn& p = it->second;
+                const int n = (int)p.ia.size();
+                group_indices(p.ia.data(), p.ja.data(), n, order, gb, gi, gj);
+                const int prim0 = (int)H.P.size();
+                for (size_t g = 0; g + 1 < gb.size(); g++) {
+                    H.ao.push_back(make_int2(gi[g], gj[g]));
+                    const int q = order[gb[g]];
+                    H.AB.push_back(make_double4(p.A[4 * q] - p.B[4 * q], p.A[4 * q + 1] - p.B[4 * q + 1],
+                                                p.A[4 * q + 2] - p.B[4 * q + 2], 0.0));
+                    H.begin.push_back(prim0 + gb[g + 1]);
+                }
+                for (int k = 0; k < n; k++) {
+                    const int q = order[k];
+                    const double* P = &p.P[4 * q];
+                    const double* A = &p.A[4 * q];
+                    H.P.push_back(make_double4(P[0], P[1], P[2], P[3]));
+                    H.PA.push_back(make_double4(P[0] - A[0], P[1] - A[1], P[2] - A[2], p.coef[q]));
+                }
+            }
+            H.sp_begin.push_back((int)H.ao.size());
+        }
+    }
+    for (auto& ac : aux_classes) {
+        KetHost& H = kh[ac.first];
+        H.begin.push_back(0);
+        H.aux_begin.push_back(0);
+        for (int m = 0; m < b->n_mol; m++) {
+            auto it = b->aux[m].find(ac.first);
+            if (it != b->aux[m].end() && !it->second.start.empty()) {
+                const AuxIn& a = it->second;
+                const int n = (int)a.start.size();
+                group_indices(a.start.data(), nullptr, n, order, gb, gi, gj);
+                const int prim0 = (int)H.C.size();
+                for (size_t g = 0; g + 1 < gb.size(); g++) {
+                    H.start.push_back(gi[g]);
+                    H.begin.push_back(prim0 + gb[g + 1]);
+                }
+                for (int k = 0; k < n; k++) {
+                    const int q = order[k];
+                    H.C.push_back(make_double4(a.C[4 * q], a.C[4 * q + 1], a.C[4 * q + 2], a.C[4 * q + 3]));
+                    H.coef.push_back(a.coef[q]);
+                }
+            }
+            H.aux_begin.push_back((int)H.start.size());
+        }
+    }
+    // ---- plans (one per pair class x aux class)
+    for (auto& pc : pair_classes)
+        for (auto& ac : aux_classes) {
+            ClassPlan pl;
+            pl.li = pc.first.first;
+            pl.lj = pc.first.second;
+            pl.lk = ac.first;
+            pl.fast = b->spherical && fast3c_supported(pl.li, pl.lj, pl.lk);
+            const BraHost& B = bh[pc.first];
+            const KetHost& K = kh[ac.first];
+            const int ni = b->spherical ? nsph(pl.li) : ncart(pl.li), nj = b->spherical ? nsph(pl.lj) : ncart(pl.lj),
+                      nk = b->spherical ? nsph(pl.lk) : ncart(pl.lk);
+            long long items = 0;
+            for (int m = 0; m < b->n_mol; m++) {
+                const int nsp = B.sp_begin[m + 1] - B.sp_begin[m], nax = K.aux_begin[m + 1] - K.aux_begin[m];
+                pl.n_sp.push_back(nsp);
+                pl.n_auxsh.push_back(nax);
+                pl.sp0.push_back(B.sp_begin[m]);
+                pl.aux0.push_back(K.aux_begin[m]);
+                pl.out_begin.push_back(b->out_elems);
+                const long long blk = (long long)nsp * ni * nj * nk * nax;
+                b->out_elems += blk;
+                pl.out_elems += blk;
+                items += (long long)nsp * ((nax + 31) / 32);
+                if (!pl.fast)
+                    b->scratch_elems = std::max(b->scratch_elems, (size_t)nsp * nax * ncart(pl.li) * ncart(pl.lj) *
+                                                                      ncart(pl.lk));
+            }
+            if (items > 0x7fffffffLL) return fail(b, "too many work items in one class", cudaSuccess);
+            pl.total_items = (int)items;
+            pl.flops_weight = (double)pl.out_elems * (pl.li + pl.lj + pl.lk + 1);
+            b->plans.push_back(pl);
+        }
+    // ---- one pinned buffer with every table, mirrored on the device
+    Layout L;
+    struct BraOff { size_t beg, ao, ab, p, pa, spb; };
+    struct KetOff { size_t beg, st, c, co, axb; };
+    std::map<std::pair<int, int>, BraOff> bo;
+    std::map<int, KetOff> ko;
+    for (auto& kv : bh) {
+        const BraHost& H = kv.second;
+        bo[kv.first] = BraOff{L.add(sizeof(int) * H.begin.size()), L.add(sizeof(int2) * H.ao.size()),
+                              L.add(sizeof(double4) * H.AB.size()), L.add(sizeof(double4) * H.P.size()),
+                              L.add(sizeof(double4) * H.PA.size()), L.add(sizeof(int) * H.sp_begin.size())};
+    }
+    for (auto& kv : kh) {
+        const KetHost& H = kv.second;
+        ko[kv.first] = KetOff{L.add(sizeof(int) * H.begin.size()), L.add(sizeof(int) * H.start.size()),
+                              L.add(sizeof(double4) * H.C.size()), L.add(sizeof(double) * H.coef.size()),
+                              L.add(sizeof(int) * H.aux_begin.size())};
+    }
+    std::vector<size_t> plan_off;
+    for (auto& pl : b->plans) {
+        plan_off.push_back(L.add(sizeof(int) * (3 * (b->n_mol + 1) + 2) + sizeof(long long) * (b->n_mol + 1)));
+    }
+    size_t etab_total = 0;
+    for (auto& kv : bh) {
+        b->etab_offset[kv.first] = etab_total;
+        etab_total += e_table_doubles(kv.first.first, kv.first.second) * kv.second.P.size();
+    }
+    b->table_bytes = L.total;
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(b, "stream", e);
+    if ((e = cudaMallocHost(&b->h_tables, L.total)) != cudaSuccess) return fail(b, "pinned tables", e);
+    if ((e = cudaMalloc(&b->d_tables, L.total)) != cudaSuccess) return fail(b, "device tables", e);
+    if ((e = cudaMalloc((void**)&b->d_etab, sizeof(double) * std::max<size_t>(etab_total, 1))) != cudaSuccess)
+        return fail(b, "E tables", e);
+    if ((e = cudaMalloc((void**)&b->d_checksum, sizeof(double) * b->n_mol)) != cudaSuccess)
+        return fail(b, "checksums", e);
+    if (b->scratch_elems && (e = cudaMalloc((void**)&b->d_scratch, sizeof(double) * b->scratch_elems)) != cudaSuccess)
+        return fail(b, "generic scratch", e);
+    void* h = b->h_tables;
+    void* d = b->d_tables;
+    for (auto& kv : bh) {
+        const BraHost& H = kv.second;
+        const BraOff& o = bo[kv.first];
+        memcpy(at<int>(h, o.beg), H.begin.data(), sizeof(int) * H.begin.size());
+        memcpy(at<int2>(h, o.ao), H.ao.data(), sizeof(int2) * H.ao.size());
+        memcpy(at<double4>(h, o.ab), H.AB.data(), sizeof(double4) * H.AB.size());
+        memcpy(at<double4>(h, o.p), H.P.data(), sizeof(double4) * H.P.size());
+        memcpy(at<double4>(h, o.pa), H.PA.data(), sizeof(double4) * H.PA.size());
+        memcpy(at<int>(h, o.spb), H.sp_begin.data(), sizeof(int) * H.sp_begin.size());
+        b->bra_by_class[kv.first] =
+            BraTable{(int)H.ao.size(), at<int>(d, o.beg), at<int2>(d, o.ao), at<double4>(d, o.ab), at<double4>(d, o.p),
+                     at<double4>(d, o.pa), b->d_etab + b->etab_offset[kv.first]};
+        b->bra_sp_begin[kv.first] = H.sp_begin;
+    }
+    std::map<int, KetTable> ket_by_class;
+    for (auto& kv : kh) {
+        const KetHost& H = kv.second;
+        const KetOff& o = ko[kv.first];
+        memcpy(at<int>(h, o.beg), H.begin.data(), sizeof(int) * H.begin.size());
+        memcpy(at<int>(h, o.st), H.start.data(), sizeof(int) * H.start.size());
+        memcpy(at<double4>(h, o.c), H.C.data(), sizeof(double4) * H.C.size());
+        memcpy(at<double>(h, o.co), H.coef.data(), sizeof(double) * H.coef.size());
+        memcpy(at<int>(h, o.axb), H.aux_begin.data(), sizeof(int) * H.aux_begin.size());
+        ket_by_class[kv.first] =
+            KetTable{(int)H.start.size(), at<int>(d, o.beg), at<int>(d, o.st), at<double4>(d, o.c), at<double>(d, o.co)};
+        b->ket_aux_begin[kv.first] = H.aux_begin;
+    }
+    for (size_t i = 0; i < b->plans.size(); i++) {
+        ClassPlan& pl = b->plans[i];
+        const int nm = b->n_mol;
+        int* hp = at<int>(h, plan_off[i]);
+        int* dp = at<int>(d, plan_off[i]);
+        int* item_begin = hp;
+        int* sp_begin = hp + (nm + 1);
+        int* aux_begin = hp + 2 * (nm + 1);
+        hp[3 * (nm + 1)] = 0;      // work counter
+        hp[3 * (nm + 1) + 1] = 0;  // kernel self-check status
+        item_begin[0] = 0;
+        for (int m = 0; m < nm; m++)
+            item_begin[m + 1] = item_begin[m] + pl.n_sp[m] * ((pl.n_auxsh[m] + 31) / 32);
+        for (int m = 0; m <= nm; m++) {
+            sp_begin[m] = b->bra_sp_begin[{pl.li, pl.lj}][m];
+            aux_begin[m] = b->ket_aux_begin[pl.lk][m];
+        }
+        // 8-byte aligned out_begin right after the ints
+        const size_t ints = 3 * (nm + 1) + 2;
+        const size_t ob_off = plan_off[i] + ((sizeof(int) * ints + 7) & ~size_t(7));
+        memcpy(at<long long>(h, ob_off), pl.out_begin.data(), sizeof(long long) * nm);
+        pl.bra = b->bra_by_class[{pl.li, pl.lj}];
+        pl.ket = ket_by_class[pl.lk];
+        pl.counter = dp + 3 * (nm + 1);
+        pl.map = BatchMap{nm, dp, dp + (nm + 1), dp + 2 * (nm + 1), at<long long>(d, ob_off), nullptr};
+    }
+    if ((e = cudaMemcpyAsync(d, h, L.total, cudaMemcpyHostToDevice, b->stream)) != cudaSuccess)
+        return fail(b, "table upload", e);
+    if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return fail(b, "table upload", e);
+    // heaviest classes first in the graph
+    std::sort(b->plans.begin(), b->plans.end(),
+              [](const ClassPlan& x, const ClassPlan& y) { return x.flops_weight > y.flops_weight; });
+    b->built = true;
+    return 0;
+}
+
+long long eip_batch_output_elems(eip_batch* b) { return b && b->built ? b->out_elems : -1; }
+
+int eip_batch_block(eip_batch* b, int mol, int i_L, int j_L, int k_L, long long* offset, int* n_pair_shells,
+                    int* n_aux_shells) {
+    if (!b || !b->built || mol < 0 || mol >= b->n_mol) return 2;
+    for (const ClassPlan& pl : b->plans)
+        if (pl.li == i_L && pl.lj == j_L && pl.lk == k_L) {
+            *offset = pl.out_begin[mol];
+            *n_pair_shells = pl.n_sp[mol];
+            *n_aux_shells = pl.n_auxsh[mol];
+            return 0;
+        }
+    return 1;
+}
+
+int eip_batch_bind_output(eip_batch* b, double* device_out) {
+    if (!b || !b->built) return 2;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+    }
+    if (b->own_out && b->d_out) cudaFree(b->d_out);
+    b->own_out = false;
+    b->d_out = device_out;
+    return 0;
+}
+
+int eip_batch_alloc_output(eip_batch* b) {
+    if (!b || !b->built) return 2;
+    double* p = nullptr;
+    cudaError_t e = cudaMalloc((void**)&p, sizeof(double) * std::max<long long>(b->out_elems, 1));
+    if (e != cudaSuccess) return fail(b, "output allocation", e);
+    eip_batch_bind_output(b, p);
+    b->own_out = true;
+    return 0;
+}
+
+double* eip_batch_output_device(eip_batch* b) { return b ? b->d_out : nullptr; }
+
+static int capture(eip_batch* b, bool checksum) {
+    cudaError_t e;
+    const int n_side = 4;
+    if (b->side.empty()) {
+        for (int i = 0; i < n_side; i++) {
+            cudaStream_t s;
+            if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess) return fail(b, "stream", e);
+            b->side.push_back(s);
+        }
+        for (int i = 0; i < 2 * n_side + 1; i++) {
+            cudaEvent_t ev;
+            if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(b, "event", e);
+            b->events.push_back(ev);
+        }
+    }
+    unsigned long long launches = 0;
+    if ((e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+        return fail(b, "begin capture", e);
+    int rc = 0;
+    cudaMemsetAsync(b->d_checksum, 0, sizeof(double) * b->n_mol, b->stream);
+    for (ClassPlan& pl : b->plans)
+        if (pl.fast) cudaMemsetAsync(pl.counter, 0, 2 * sizeof(int), b->stream);
+    for (auto& kv : b->bra_by_class) {
+        if (!fast3c_supported(kv.first.first, kv.first.second, 0) || !b->spherical) continue;
+        rc |= launch_e_table(kv.first.first, kv.first.second, kv.second, b->d_etab + b->etab_offset[kv.first],
+                             b->stream);
+        launches++;
+    }
+    cudaEventRecord(b->events[0], b->stream);
+    for (int i = 0; i < n_side; i++) cudaStreamWaitEvent(b->side[i], b->events[0], 0);
+    int next = 0;
+    for (ClassPlan& pl : b->plans) {
+        if (pl.total_items == 0) continue;
+        cudaStream_t s = b->side[next++ % n_side];
+        if (pl.fast) {
+            BatchMap map = pl.map;
+            map.checksum = checksum ? b->d_checksum : nullptr;
+            rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, map, pl.total_items, b->omega, b->d_out,
+                                pl.counter, s);
+            launches++;
+        } else {
+            for (int m = 0; m < b->n_mol; m++) {
+                if (pl.n_sp[m] == 0 || pl.n_auxsh[m] == 0) continue;
+                BraTable bra = pl.bra;
+                bra.n_group = pl.n_sp[m];
+                bra.grp_begin += pl.sp0[m];
+                bra.grp_ao += pl.sp0[m];
+                bra.grp_AB += pl.sp0[m];
+                KetTable ket = pl.ket;
+                ket.n_group = pl.n_auxsh[m];
+                ket.grp_begin += pl.aux0[m];
+                ket.grp_start += pl.aux0[m];
+                rc |= launch_generic_raw(0, pl.li, pl.lj, pl.lk, bra, ket, b->omega, 0, b->d_scratch, s);
+                rc |= launch_transform(pl.li, pl.lj, pl.lk, b->spherical, pl.n_sp[m], pl.n_auxsh[m], b->d_scratch,
+                                       b->d_out + pl.out_begin[m], s);
+                launches += 2;
+            }
+        }
+    }
+    for (int i = 0; i < n_side; i++) {
+        cudaEventRecord(b->events[1 + i], b->side[i]);
+        cudaStreamWaitEvent(b->stream, b->events[1 + i], 0);
+    }
+    e = cudaStreamEndCapture(b->stream, &b->graph);
+    if (e != cudaSuccess || rc != 0) return fail(b, "graph capture", e);
+    if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess) return fail(b, "graph instantiate", e);
+    b->launches_per_run = launches;
+    return 0;
+}
+
+int eip_batch_run(eip_batch* b, int checksum) {
+    if (!b || !b->built || !b->d_out) return 2;
+    if (!b->exec) {
+        if (int rc = capture(b, checksum != 0)) return rc;
+    }
+    cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
+    if (e != cudaSuccess) return fail(b, "graph launch", e);
+    return 0;
+}
+
+int eip_batch_run_class(eip_batch* b, int i_L, int j_L, int k_L) {
+    if (!b || !b->built || !b->d_out) return 2;
+    for (ClassPlan& pl : b->plans) {
+        if (pl.li != i_L || pl.lj != j_L || pl.lk != k_L) continue;
+        if (!pl.fast || pl.total_items == 0) return 1;
+        cudaMemsetAsync(pl.counter, 0, 2 * sizeof(int), b->stream);
+        int rc = launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, pl.map, pl.total_items, b->omega, b->d_out,
+                               pl.counter, b->stream);
+        return rc == 0 ? 0 : fail(b, "class launch", cudaGetLastError());
+    }
+    return 1;
+}
+
+int eip_batch_upload(eip_batch* b) {
+    if (!b || !b->built) return 2;
+    cudaError_t e = cudaMemcpyAsync(b->d_tables, b->h_tables, b->table_bytes, cudaMemcpyHostToDevice, b->stream);
+    return e == cudaSuccess ? 0 : fail(b, "table upload", e);
+}
+
+long long eip_batch_table_bytes(eip_batch* b) { return b && b->built ? (long long)b->table_bytes : -1; }
+
+unsigned long long eip_batch_launches_per_run(eip_batch* b) { return b ? b->launches_per_run : 0; }
+
+int eip_batch_checksums(eip_batch* b, double* host) {
+    if (!b || !b->built) return 2;
+    cudaError_t e = cudaMemcpyAsync(host, b->d_checksum, sizeof(double) * b->n_mol, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? 0 : fail(b, "checksum copy", e);
+}
+
+int eip_batch_sync(eip_batch* b) {
+    if (!b || !b->built) return 2;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? 0 : fail(b, "batch kernels", e);
+}
+
+int eip_batch_status(eip_batch* b) {
+    if (!b || !b->built) return 2;
+    for (const ClassPlan& pl : b->plans) {
+        if (!pl.fast) continue;
+        int st[2] = {0, 0};
+        cudaError_t e = cudaMemcpyAsync(st, pl.counter, sizeof(st), cudaMemcpyDeviceToHost, b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) return fail(b, "status copy", e);
+        if (st[1] != 0) {
+            snprintf(b->err, sizeof b->err, "class (%d%d|%d) kernel self-check %d", pl.li, pl.lj, pl.lk, st[1]);
+            return 3;
+        }
+    }
+    return 0;
+}
+
+void* eip_batch_stream(eip_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+int eip_batch_copy_output(eip_batch* b, long long offset, long long count, double* host) {
+    if (!b || !b->built || !b->d_out || offset < 0 || count < 0 || offset + count > b->out_elems) return 2;
+    cudaError_t e = cudaMemcpyAsync(host, b->d_out + offset, sizeof(double) * count, cudaMemcpyDeviceToHost,
+                                    b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? 0 : fail(b, "output copy", e);
+}
+
+void eip_batch_destroy(eip_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->own_out && b->d_out) cudaFree(b->d_out);
+    if (b->d_tables) cudaFree(b->d_tables);
+    if (b->h_tables) cudaFreeHost(b->h_tables);
+    if (b->d_etab) cudaFree(b->d_etab);
+    if (b->d_checksum) cudaFree(b->d_checksum);
+    if (b->d_scratch) cudaFree(b->d_scratch);
+    for (auto s : b->side) cudaStreamDestroy(s);
+    for (auto ev : b->events) cudaEventDestroy(ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+}  // extern "C"

@@ -217,6 +217,25 @@ struct BraTable {
     const double4* grp_AB;
     const double4* prim_P;
     const double4* prim_PA;
+    // Optional: per primitive pair, the x, y and z tables E^{i,j}_t
+    // (3 * e_size<LI,LJ>() doubles, fast (mu nu|P) kernels only).
+    const double* prim_E;
+};
+
+// Work map of one (l_i, l_j | l_k) class over a batch of molecules.
+// Molecule m owns shell pairs [sp_begin[m], sp_begin[m+1]) of the class's
+// bra table and auxiliary shells [aux_begin[m], aux_begin[m+1]) of its ket
+// table.  Its work items are (shell pair, tile of 32 auxiliary shells),
+// numbered from item_begin[m]; its packed output block starts at element
+// out_begin[m].  checksum (optional) receives the sum of every value written
+// for molecule m.
+struct BatchMap {
+    int n_mol;
+    const int* item_begin;  // n_mol + 1
+    const int* sp_begin;    // n_mol + 1
+    const int* aux_begin;   // n_mol + 1
+    const long long* out_begin;
+    double* checksum;
 };
 
 // One-centre ("ket") table: auxiliary shells of one class (or point charges).

@@ -8,6 +8,7 @@ namespace eip {
 
 struct BraTable;
 struct KetTable;
+struct BatchMap;
 
 int upload_constant_tables();
 int upload_generic_tables();
@@ -15,8 +16,10 @@ const double* boys_table_device();
 int launch_boys_probe(int L, const double* dT, int n, double* dout, cudaStream_t s);
 
 bool fast3c_supported(int li, int lj, int lk);
-int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& ket, double omega, double* out,
-                  cudaStream_t s);
+size_t e_table_doubles(int li, int lj);
+int launch_e_table(int li, int lj, const BraTable& bra, double* prim_E, cudaStream_t s);
+int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& ket, const BatchMap& map,
+                  int total_items, double omega, double* out, int* counter, cudaStream_t s);
 
 int generic_kc_chunk(int li, int lj, int lk);
 size_t generic_smem_bytes(int li, int lj, int lk, int kc_chunk);

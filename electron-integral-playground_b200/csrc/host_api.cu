@@ -73,7 +73,7 @@ struct Context {
     int device = -1;
     cudaStream_t stream = nullptr;
     PinnedBuffer h_in, h_out;
-    DeviceBuffer d_in, d_raw, d_out;
+    DeviceBuffer d_in, d_raw, d_out, d_etab, d_misc;
     unsigned long long launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_kernel_ms = 0.0f;  // device time of the last class's kernels
@@ -156,6 +156,7 @@ struct Staged {
     BraTable bra{};
     KetTable ket{};
     const double* prim_b = nullptr;
+    int n_bra_prims = 0;
 };
 
 template <typename T>
@@ -260,7 +261,8 @@ int stage_inputs(Context& c, const BraInput& bi, const KetInput& ki, Staged& st,
     }
     void* d = c.d_in.ptr;
     st.bra = BraTable{nb, at<int>(d, o_bbeg), at<int2>(d, o_bao), at<double4>(d, o_bab), at<double4>(d, o_bp),
-                      at<double4>(d, o_bpa)};
+                      at<double4>(d, o_bpa), nullptr};
+    st.n_bra_prims = npb;
     st.prim_b = at<double>(d, o_bb);
     st.ket = KetTable{nk, at<int>(d, o_kbeg), at<int>(d, o_kst), at<double4>(d, o_kc), at<double>(d, o_kco)};
     return 0;
@@ -281,8 +283,40 @@ int compute_class(Context& c, int mode, int li, int lj, int lk, bool spherical, 
     const int n_bra = st.bra.n_group, n_ket = mode == 3 ? 1 : st.ket.n_group;
     cudaEventRecord(c.ev0, c.stream);
     if (mode == 0 && spherical && fast3c_supported(li, lj, lk)) {
-        rc = launch_fast3c(li, lj, lk, st.bra, st.ket, omega, dout, c.stream);
-        c.launches += 1;
+        // A batch of one molecule: E tables, then the persistent class kernel.
+        const int n_tiles = (n_ket + 31) / 32;
+        const long long items = (long long)n_bra * n_tiles;
+        if (items > 0x7fffffffLL) {
+            set_error("class too large for one call", cudaSuccess);
+            return 2;
+        }
+        const int n_pp = st.n_bra_prims;
+        e = c.d_etab.reserve(sizeof(double) * e_table_doubles(li, lj) * (size_t)n_pp);
+        if (e == cudaSuccess) e = c.d_misc.reserve(256);
+        if (e != cudaSuccess) {
+            set_error("E-table allocation", e);
+            return 2;
+        }
+        BraTable bra = st.bra;
+        bra.prim_E = static_cast<double*>(c.d_etab.ptr);
+        int* misc = static_cast<int*>(c.d_misc.ptr);  // [0] counter, [4..5] item_begin, [8..9] sp, [12..13] aux
+        const int host_misc[16] = {0, 0, 0, 0, 0, (int)items, 0, 0, 0, n_bra, 0, 0, 0, n_ket, 0, 0};
+        cudaMemcpyAsync(misc, host_misc, sizeof(host_misc), cudaMemcpyHostToDevice, c.stream);
+        long long* out_begin = reinterpret_cast<long long*>(misc + 16);
+        cudaMemsetAsync(out_begin, 0, sizeof(long long), c.stream);
+        BatchMap map{1, misc + 4, misc + 8, misc + 12, out_begin, nullptr};
+        rc = launch_e_table(li, lj, bra, static_cast<double*>(c.d_etab.ptr), c.stream);
+        if (rc == 0) rc = launch_fast3c(li, lj, lk, bra, st.ket, map, (int)items, omega, dout, misc, c.stream);
+        c.launches += 2;
+        int status[2] = {0, 0};
+        if (rc == 0) e = cudaMemcpyAsync(status, misc, sizeof(status), cudaMemcpyDeviceToHost, c.stream);
+        if (rc == 0 && e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+        if (rc == 0 && (e != cudaSuccess || status[1] != 0)) {
+            snprintf(g_last_error, sizeof g_last_error, "fast (mu nu|P) kernel self-check %d (cuda: %s)", status[1],
+                     cudaGetErrorString(e));
+            fprintf(stderr, "[eip] %s\n", g_last_error);
+            return 2;
+        }
     } else {
         const size_t n_raw = (size_t)n_bra * n_ket * ncart(li) * ncart(lj) * ncart(lk);
         e = c.d_raw.reserve(sizeof(double) * n_raw);

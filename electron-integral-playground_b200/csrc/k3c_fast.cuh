@@ -7,16 +7,23 @@
 // (reference: MI/three_center.cpp:10-26 for the formula, :27-173 for one
 // primitive triplet; erf-attenuated variant for omega > 0, :46-49).
 //
-// Mapping (this library's design, not the reference's): one CTA handles one
-// shell pair and 32 auxiliary shells, lane = auxiliary shell, so the final
-// stores of each warp are 32 consecutive doubles.  The KS warps of the CTA
-// split (a) the entries of the Hermite tetrahedron R_{tuv} (closed form from
-// R^{(m)}_000, written to shared memory) and (b) the spherical ket
-// components; the ket Cartesian->spherical transform and the one-centre
-// Hermite coefficients are folded into compile-time constants.  Primitive
-// pairs are reduced in registers: each contracted block is written once, with
-// no atomics.  Output layout ("packed"):
-//   out[((pair * nsph_i * nsph_j + I * nsph_j + J) * nsph_k + K) * n_aux_shell + P]
+// Mapping (this library's design, not the reference's):
+//   * persistent CTAs take work items (shell pair, 32 auxiliary shells) of a
+//     multi-molecule work list from an atomic counter;
+//   * lane = auxiliary shell, so the stores of a warp are 32 consecutive doubles;
+//   * the KS warps of a CTA split (a) the entries of the Hermite tetrahedron
+//     R_{tuv} (closed form from R^{(m)}_000, shared through shared memory) and
+//     (b) the spherical ket components; a warp evaluates its KPW ket
+//     components together so every shared-memory E^{ij}_t load feeds KPW FMAs;
+//   * the ket Cartesian->spherical transform and one-centre Hermite
+//     coefficients are compile-time constants (zero terms vanish);
+//   * E^{ij}_t tables of each primitive pair are precomputed once into the
+//     device-resident pair table (e_table_kernel) and staged per pair into
+//     shared memory;
+//   * primitive pairs are reduced in registers: each contracted block is
+//     written once, with no atomics.
+// Packed output of molecule m (element offset out_begin[m]):
+//   out[((pair * nsph_i * nsph_j + I * nsph_j + J) * nsph_k + K) * n_aux_shell_m + P]
 #pragma once
 
 #include "eip_common.cuh"
@@ -31,6 +38,7 @@ struct Fast3c {
     static constexpr int L = LI + LJ + LK;
     static constexpr int LIJ = LI + LJ;
     static constexpr int NI = ncart(LI), NJ = ncart(LJ), NIJ = NI * NJ;
+    static constexpr int NIJS = nsph(LI) * nsph(LJ);
     static constexpr int NKO = nsph(LK);
     static constexpr int KPW_MAX = (kAccMax / NIJ) < 1 ? 1 : (kAccMax / NIJ);
     static constexpr int KS = (NKO + KPW_MAX - 1) / KPW_MAX;  // warps per CTA
@@ -80,232 +88,339 @@ __device__ __forceinline__ void bra_e_table(double PA, double AB, double inv2p, 
             for (int t = 0; t <= i + j; t++) out[e_offset<LJ>(i, j) + t] = W[i][j][t];
 }
 
+// Fill bra.prim_E: one thread per shell pair, looping over its primitive pairs.
+template <int LI, int LJ>
+__global__ void e_table_kernel(BraTable bra, double* __restrict__ prim_E) {
+    constexpr int NE = e_size<LI, LJ>();
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= bra.n_group) return;
+    const double4 AB = bra.grp_AB[g];
+    for (int pp = bra.grp_begin[g]; pp < bra.grp_begin[g + 1]; pp++) {
+        const double4 PA = bra.prim_PA[pp];
+        const double inv2p = 0.5 / bra.prim_P[pp].w;
+        double* out = prim_E + (size_t)pp * 3 * NE;
+        bra_e_table<LI, LJ>(PA.x, AB.x, inv2p, out);
+        bra_e_table<LI, LJ>(PA.y, AB.y, inv2p, out + NE);
+        bra_e_table<LI, LJ>(PA.z, AB.z, inv2p, out + 2 * NE);
+    }
+}
+
 template <int LI, int LJ, int LK>
 __global__ void __launch_bounds__(Fast3c<LI, LJ, LK>::THREADS)
-k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, int n_tiles, double omega,
-         double* __restrict__ out) {
+k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, BatchMap map, double omega,
+         double* __restrict__ out, int* __restrict__ work_counter, int total_items) {
     using C = Fast3c<LI, LJ, LK>;
     constexpr int L = C::L;
     __shared__ double sE[3 * C::NE];
     __shared__ double sR[C::NR * 32];
+    __shared__ int s_item;
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int sp = blockIdx.x / n_tiles;
-    const int tile = blockIdx.x - sp * n_tiles;
-    const int a = tile * 32 + lane;
-    const bool valid = a < ket.n_group;
-    int kb = 0, nk = 0;
-    if (valid) {
-        kb = ket.grp_begin[a];
-        nk = ket.grp_begin[a + 1] - kb;
-    }
-    const int nk_max = __reduce_max_sync(0xffffffffu, nk);
-    const int pb = bra.grp_begin[sp], pe = bra.grp_begin[sp + 1];
-    const double4 AB = bra.grp_AB[sp];
+    // work_counter[0]: next item; work_counter[1]: status (0 ok, else the
+    // first failed self-check: 1 loop bound, 2 molecule/pair index, 3 pair or
+    // auxiliary primitive count out of range).
+    int* status = work_counter + 1;
 
-    double acc[C::NIJ][C::KPW];
-#pragma unroll
-    for (int i = 0; i < C::NIJ; i++)
-#pragma unroll
-        for (int c = 0; c < C::KPW; c++) acc[i][c] = 0.0;
-
-    for (int pp = pb; pp < pe; pp++) {
-        const double4 P = bra.prim_P[pp];
-        const double4 PA = bra.prim_PA[pp];
-        const double p = P.w;
-        if (warp == 0 && lane < 3) {
-            const double pa = lane == 0 ? PA.x : (lane == 1 ? PA.y : PA.z);
-            const double ab = lane == 0 ? AB.x : (lane == 1 ? AB.y : AB.z);
-            bra_e_table<LI, LJ>(pa, ab, 0.5 / p, sE + lane * C::NE);
+    for (int iter = 0;; iter++) {
+        if (threadIdx.x == 0) s_item = atomicAdd(work_counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= total_items || item < 0) return;
+        if (iter > total_items) {  // a CTA can never take more items than exist
+            if (threadIdx.x == 0) atomicCAS(status, 0, 1);
+            return;
         }
-        for (int kk = 0; kk < nk_max; kk++) {
-            const bool live = kk < nk;
-            const double4 Cq = live ? ket.prim_C[kb + kk] : make_double4(P.x, P.y, P.z, 1.0);
-            const double cc = live ? ket.prim_coef[kb + kk] : 0.0;
-            const double q = Cq.w;
-            const double X = P.x - Cq.x, Y = P.y - Cq.y, Z = P.z - Cq.z;
-            double zeta, pref;
-            if (omega == 0.0) {
-                zeta = p * q / (p + q);
-                pref = PA.w * cc * kTwoPi52 / (p * q * sqrt(p + q));
-            } else {
-                zeta = 1.0 / (1.0 / p + 1.0 / q + 1.0 / (omega * omega));
-                pref = PA.w * cc * kTwoPi52 * omega / (p * q * sqrt(p * q + (p + q) * omega * omega));
-            }
-            if (LK & 1) pref = -pref;  // (-1)^{|s|} with |s| = LK mod 2
 
-            // R^{(m)}_000 = (-2 zeta)^m F_m(zeta |PQ|^2), then this warp's share of
-            // the tetrahedron by the closed form (per-entry independent).
-            double Rm[L + 1];
-            boys<L>(boys_table, zeta * (X * X + Y * Y + Z * Z), Rm);
-            {
-                double f = -2.0 * zeta, g = f;
+        // molecule of this item: last m with item_begin[m] <= item
+        int lo = 0, hi = map.n_mol - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(map.item_begin + mid) <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const int m = lo;
+        const int aux0 = __ldg(map.aux_begin + m);
+        const int n_aux = __ldg(map.aux_begin + m + 1) - aux0;
+        const int n_tiles = (n_aux + 31) >> 5;
+        const int local = item - __ldg(map.item_begin + m);
+        const int sp_local = local / n_tiles;
+        const int tile = local - sp_local * n_tiles;
+        const int sp = __ldg(map.sp_begin + m) + sp_local;
+        const int a_local = tile * 32 + lane;
+        const bool valid = a_local < n_aux;
+        const int a = aux0 + a_local;
+
+        int kb = 0, nk = 0;
+        if (valid) {
+            kb = __ldg(ket.grp_begin + a);
+            nk = __ldg(ket.grp_begin + a + 1) - kb;
+        }
+        const int nk_max = __reduce_max_sync(0xffffffffu, nk);
+        if (m < 0 || m >= map.n_mol || sp_local < 0 || sp < 0 || sp >= bra.n_group || n_tiles <= 0) {
+            if (threadIdx.x == 0) atomicCAS(status, 0, 2);
+            continue;  // every value tested here is the same for all threads of the CTA
+        }
+        const int pb = __ldg(bra.grp_begin + sp), pe = __ldg(bra.grp_begin + sp + 1);
+        if (pe < pb || pe - pb > 4096 || nk_max < 0 || nk_max > 4096) {
+            if (threadIdx.x == 0) atomicCAS(status, 0, 3);
+            continue;
+        }
+
+        double acc[C::NIJ][C::KPW];
 #pragma unroll
-                for (int m = 1; m <= L; m++) {
-                    Rm[m] *= g;
-                    g *= f;
+        for (int i = 0; i < C::NIJ; i++)
+#pragma unroll
+            for (int c = 0; c < C::KPW; c++) acc[i][c] = 0.0;
+
+        for (int pp = pb; pp < pe; pp++) {
+            const double4 P = bra.prim_P[pp];
+            const double4 PA = bra.prim_PA[pp];
+            const double p = P.w;
+            for (int e = threadIdx.x; e < 3 * C::NE; e += C::THREADS)
+                sE[e] = __ldg(bra.prim_E + (size_t)pp * 3 * C::NE + e);
+            for (int kk = 0; kk < nk_max; kk++) {
+                const bool live = kk < nk;
+                const double4 Cq = live ? ket.prim_C[kb + kk] : make_double4(P.x, P.y, P.z, 1.0);
+                const double cc = live ? ket.prim_coef[kb + kk] : 0.0;
+                const double q = Cq.w;
+                const double X = P.x - Cq.x, Y = P.y - Cq.y, Z = P.z - Cq.z;
+                double zeta, pref;
+                if (omega == 0.0) {
+                    zeta = p * q / (p + q);
+                    pref = PA.w * cc * kTwoPi52 / (p * q * sqrt(p + q));
+                } else {
+                    zeta = 1.0 / (1.0 / p + 1.0 / q + 1.0 / (omega * omega));
+                    pref = PA.w * cc * kTwoPi52 * omega / (p * q * sqrt(p * q + (p + q) * omega * omega));
                 }
-            }
-            double px[L + 1], py[L + 1], pz[L + 1];
-            px[0] = py[0] = pz[0] = 1.0;
+                if (LK & 1) pref = -pref;  // (-1)^{|s|} with |s| = LK mod 2
+
+                // R^{(m)}_000 = (-2 zeta)^m F_m(zeta |PQ|^2); this warp's share of
+                // the tetrahedron by the closed form (entries are independent).
+                double Rm[L + 1];
+                boys<L>(boys_table, zeta * (X * X + Y * Y + Z * Z), Rm);
+                {
+                    const double f = -2.0 * zeta;
+                    double g = f;
 #pragma unroll
-            for (int m = 1; m <= L; m++) {
-                px[m] = px[m - 1] * X;
-                py[m] = py[m - 1] * Y;
-                pz[m] = pz[m - 1] * Z;
-            }
-            static_for<0, C::KS>([&](auto g) {
-                constexpr int G = decltype(g)::value;
-                constexpr int lo = G * C::RPW;
-                constexpr int hi = (G + 1) * C::RPW < C::NR ? (G + 1) * C::RPW : C::NR;
-                if (warp == G) {
-                    static_for<lo, hi>([&](auto e) {
-                        constexpr int idx = decltype(e)::value;
-                        constexpr int t = herm_t(idx), u = herm_u(idx), v = herm_v(idx);
-                        double r = 0.0;
-                        static_for<(t + 1) / 2, t + 1>([&](auto mx_) {
-                            constexpr int mx = decltype(mx_)::value;
-                            double ry = 0.0;
-                            static_for<(u + 1) / 2, u + 1>([&](auto my_) {
-                                constexpr int my = decltype(my_)::value;
-                                double rz = 0.0;
-                                static_for<(v + 1) / 2, v + 1>([&](auto mz_) {
-                                    constexpr int mz = decltype(mz_)::value;
-                                    constexpr double h = hermite_r_coef(v, mz);
-                                    rz = fma(h * pz[2 * mz - v], Rm[mx + my + mz], rz);
+                    for (int mm = 1; mm <= L; mm++) {
+                        Rm[mm] *= g;
+                        g *= f;
+                    }
+                }
+                double px[L + 1], py[L + 1], pz[L + 1];
+                px[0] = py[0] = pz[0] = 1.0;
+#pragma unroll
+                for (int mm = 1; mm <= L; mm++) {
+                    px[mm] = px[mm - 1] * X;
+                    py[mm] = py[mm - 1] * Y;
+                    pz[mm] = pz[mm - 1] * Z;
+                }
+                static_for<0, C::KS>([&](auto g) {
+                    constexpr int G = decltype(g)::value;
+                    constexpr int lo_e = G * C::RPW;
+                    constexpr int hi_e = (G + 1) * C::RPW < C::NR ? (G + 1) * C::RPW : C::NR;
+                    if (warp == G) {
+                        static_for<lo_e, hi_e>([&](auto e) {
+                            constexpr int idx = decltype(e)::value;
+                            constexpr int t = herm_t(idx), u = herm_u(idx), v = herm_v(idx);
+                            double r = 0.0;
+                            static_for<(t + 1) / 2, t + 1>([&](auto mx_) {
+                                constexpr int mx = decltype(mx_)::value;
+                                double ry = 0.0;
+                                static_for<(u + 1) / 2, u + 1>([&](auto my_) {
+                                    constexpr int my = decltype(my_)::value;
+                                    double rz = 0.0;
+                                    static_for<(v + 1) / 2, v + 1>([&](auto mz_) {
+                                        constexpr int mz = decltype(mz_)::value;
+                                        constexpr double h = hermite_r_coef(v, mz);
+                                        rz = fma(h * pz[2 * mz - v], Rm[mx + my + mz], rz);
+                                    });
+                                    constexpr double h = hermite_r_coef(u, my);
+                                    ry = fma(h * py[2 * my - u], rz, ry);
                                 });
-                                constexpr double h = hermite_r_coef(u, my);
-                                ry = fma(h * py[2 * my - u], rz, ry);
+                                constexpr double h = hermite_r_coef(t, mx);
+                                r = fma(h * px[2 * mx - t], ry, r);
                             });
-                            constexpr double h = hermite_r_coef(t, mx);
-                            r = fma(h * px[2 * mx - t], ry, r);
+                            sR[idx * 32 + lane] = r;
                         });
-                        sR[idx * 32 + lane] = r;
-                    });
-                }
-            });
-            // (1/2q)^{LK - j} weights of |s| = LK - 2j
-            double w[LK / 2 + 1];
-            {
-                const double inv2q = 0.5 / q;
-                double base = 1.0;
+                    }
+                });
+                // (1/2q)^{LK - j}: weight of the ket terms with |s| = LK - 2j
+                double w[LK / 2 + 1];
+                {
+                    const double inv2q = 0.5 / q;
+                    double base = 1.0;
 #pragma unroll
-                for (int j = 0; j < LK - LK / 2; j++) base *= inv2q;
-                // base = (1/2q)^{ceil(LK/2)} = weight of j = LK/2
+                    for (int j = 0; j < LK - LK / 2; j++) base *= inv2q;
 #pragma unroll
-                for (int j = LK / 2; j >= 0; j--) {
-                    w[j] = base;
-                    base *= inv2q;
+                    for (int j = LK / 2; j >= 0; j--) {
+                        w[j] = base;
+                        base *= inv2q;
+                    }
                 }
-            }
-            __syncthreads();
+                __syncthreads();
 
-            static_for<0, C::KS>([&](auto g) {
-                constexpr int G = decltype(g)::value;
-                if (warp == G) {
-                    static_for<0, C::KPW>([&](auto c_) {
-                        constexpr int c = decltype(c_)::value;
-                        constexpr int ko = G * C::KPW + c;
-                        if constexpr (ko < C::NKO) {
-                            double Xh[C::NHB];
-                            static_for<0, C::NHB>([&](auto h_) {
-                                constexpr int h = decltype(h_)::value;
-                                constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
-                                double xs = 0.0;
-                                static_for<0, LK / 2 + 1>([&](auto j_) {
-                                    constexpr int j = decltype(j_)::value;
-                                    constexpr int S = LK - 2 * j;
-                                    double part = 0.0;
-                                    static_for<0, ncart(S)>([&](auto sc_) {
-                                        constexpr int sc = decltype(sc_)::value;
-                                        constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
-                                        constexpr double kc = ket_sph_coef(LK, ko, sx, sy, sz);
-                                        if constexpr (kc != 0.0)
-                                            part = fma(kc, sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane], part);
-                                    });
-                                    xs = fma(w[j], part, xs);
-                                });
-                                Xh[h] = xs;
-                            });
-                            static_for<0, C::NI>([&](auto ci_) {
-                                constexpr int ci = decltype(ci_)::value;
-                                constexpr int ix = cart_x(LI, ci), iy = cart_y(LI, ci), iz = cart_z(LI, ci);
-                                static_for<0, C::NJ>([&](auto cj_) {
-                                    constexpr int cj = decltype(cj_)::value;
-                                    constexpr int jx = cart_x(LJ, cj), jy = cart_y(LJ, cj), jz = cart_z(LJ, cj);
-                                    double s = 0.0;
-                                    static_for<0, ix + jx + 1>([&](auto t_) {
-                                        constexpr int t = decltype(t_)::value;
-                                        double su = 0.0;
-                                        static_for<0, iy + jy + 1>([&](auto u_) {
-                                            constexpr int u = decltype(u_)::value;
-                                            double sv = 0.0;
-                                            static_for<0, iz + jz + 1>([&](auto v_) {
-                                                constexpr int v = decltype(v_)::value;
-                                                sv = fma(sE[2 * C::NE + e_offset<LJ>(iz, jz) + v], Xh[herm_index(t, u, v)], sv);
-                                            });
-                                            su = fma(sE[C::NE + e_offset<LJ>(iy, jy) + u], sv, su);
+                static_for<0, C::KS>([&](auto g) {
+                    constexpr int G = decltype(g)::value;
+                    constexpr int KO0 = G * C::KPW;
+                    constexpr int NC = (KO0 + C::KPW <= C::NKO) ? C::KPW : (C::NKO - KO0);
+                    if (warp == G) {
+                        // ket: X[c][h] = sum_j w_j sum_{|s| = LK-2j} K[ko][s] R[h + s]
+                        double Xh[NC][C::NHB];
+                        static_for<0, C::NHB>([&](auto h_) {
+                            constexpr int h = decltype(h_)::value;
+                            constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
+                            double xs[NC];
+#pragma unroll
+                            for (int c = 0; c < NC; c++) xs[c] = 0.0;
+                            static_for<0, LK / 2 + 1>([&](auto j_) {
+                                constexpr int j = decltype(j_)::value;
+                                constexpr int S = LK - 2 * j;
+                                double part[NC];
+#pragma unroll
+                                for (int c = 0; c < NC; c++) part[c] = 0.0;
+                                static_for<0, ncart(S)>([&](auto sc_) {
+                                    constexpr int sc = decltype(sc_)::value;
+                                    constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
+                                    constexpr bool any = [] {
+                                        for (int c = 0; c < NC; c++)
+                                            if (ket_sph_coef(LK, KO0 + c, sx, sy, sz) != 0.0) return true;
+                                        return false;
+                                    }();
+                                    if constexpr (any) {
+                                        const double r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
+                                        static_for<0, NC>([&](auto c_) {
+                                            constexpr int c = decltype(c_)::value;
+                                            constexpr double kc = ket_sph_coef(LK, KO0 + c, sx, sy, sz);
+                                            if constexpr (kc != 0.0) part[c] = fma(kc, r, part[c]);
                                         });
-                                        s = fma(sE[e_offset<LJ>(ix, jx) + t], su, s);
-                                    });
-                                    acc[ci * C::NJ + cj][c] = fma(pref, s, acc[ci * C::NJ + cj][c]);
+                                    }
                                 });
+#pragma unroll
+                                for (int c = 0; c < NC; c++) xs[c] = fma(w[j], part[c], xs[c]);
                             });
-                        }
-                    });
-                }
-            });
-            __syncthreads();
-        }
-    }
-
-    if (!valid) return;
-    const size_t n_ket = (size_t)ket.n_group;
-    static_for<0, C::KS>([&](auto g) {
-        constexpr int G = decltype(g)::value;
-        if (warp == G) {
-            static_for<0, C::KPW>([&](auto c_) {
-                constexpr int c = decltype(c_)::value;
-                constexpr int ko = G * C::KPW + c;
-                if constexpr (ko < C::NKO) {
-                    static_for<0, nsph(LI)>([&](auto I_) {
-                        constexpr int I = decltype(I_)::value;
-                        static_for<0, nsph(LJ)>([&](auto J_) {
-                            constexpr int J = decltype(J_)::value;
-                            double v = 0.0;
-                            static_for<0, C::NI>([&](auto ci_) {
-                                constexpr int ci = decltype(ci_)::value;
-                                constexpr double wi = sph_coef(LI, I, ci);
-                                if constexpr (wi != 0.0) {
-                                    double vj = 0.0;
-                                    static_for<0, C::NJ>([&](auto cj_) {
-                                        constexpr int cj = decltype(cj_)::value;
-                                        constexpr double wj = sph_coef(LJ, J, cj);
-                                        if constexpr (wj != 0.0) vj = fma(wj, acc[ci * C::NJ + cj][c], vj);
+#pragma unroll
+                            for (int c = 0; c < NC; c++) Xh[c][h] = xs[c];
+                        });
+                        // bra: acc[ij][c] += pref * sum_t Ex sum_u Ey sum_v Ez X[c][tuv]
+                        static_for<0, C::NI>([&](auto ci_) {
+                            constexpr int ci = decltype(ci_)::value;
+                            constexpr int ix = cart_x(LI, ci), iy = cart_y(LI, ci), iz = cart_z(LI, ci);
+                            static_for<0, C::NJ>([&](auto cj_) {
+                                constexpr int cj = decltype(cj_)::value;
+                                constexpr int jx = cart_x(LJ, cj), jy = cart_y(LJ, cj), jz = cart_z(LJ, cj);
+                                double s[NC];
+#pragma unroll
+                                for (int c = 0; c < NC; c++) s[c] = 0.0;
+                                static_for<0, ix + jx + 1>([&](auto t_) {
+                                    constexpr int t = decltype(t_)::value;
+                                    double su[NC];
+#pragma unroll
+                                    for (int c = 0; c < NC; c++) su[c] = 0.0;
+                                    static_for<0, iy + jy + 1>([&](auto u_) {
+                                        constexpr int u = decltype(u_)::value;
+                                        double sv[NC];
+#pragma unroll
+                                        for (int c = 0; c < NC; c++) sv[c] = 0.0;
+                                        static_for<0, iz + jz + 1>([&](auto v_) {
+                                            constexpr int v = decltype(v_)::value;
+                                            const double ez = sE[2 * C::NE + e_offset<LJ>(iz, jz) + v];
+#pragma unroll
+                                            for (int c = 0; c < NC; c++)
+                                                sv[c] = fma(ez, Xh[c][herm_index(t, u, v)], sv[c]);
+                                        });
+                                        const double ey = sE[C::NE + e_offset<LJ>(iy, jy) + u];
+#pragma unroll
+                                        for (int c = 0; c < NC; c++) su[c] = fma(ey, sv[c], su[c]);
                                     });
-                                    v = fma(wi, vj, v);
+                                    const double ex = sE[e_offset<LJ>(ix, jx) + t];
+#pragma unroll
+                                    for (int c = 0; c < NC; c++) s[c] = fma(ex, su[c], s[c]);
+                                });
+#pragma unroll
+                                for (int c = 0; c < NC; c++)
+                                    acc[ci * C::NJ + cj][c] = fma(pref, s[c], acc[ci * C::NJ + cj][c]);
+                            });
+                        });
+                    }
+                });
+                __syncthreads();
+            }
+        }
+
+        // Epilogue: bra Cartesian -> spherical, coalesced packed stores.
+        const size_t obase = (size_t)__ldg(map.out_begin + m);
+        double wsum = 0.0;
+        static_for<0, C::KS>([&](auto g) {
+            constexpr int G = decltype(g)::value;
+            if (warp == G) {
+                static_for<0, C::KPW>([&](auto c_) {
+                    constexpr int c = decltype(c_)::value;
+                    constexpr int ko = G * C::KPW + c;
+                    if constexpr (ko < C::NKO) {
+                        static_for<0, nsph(LI)>([&](auto I_) {
+                            constexpr int I = decltype(I_)::value;
+                            static_for<0, nsph(LJ)>([&](auto J_) {
+                                constexpr int J = decltype(J_)::value;
+                                double v = 0.0;
+                                static_for<0, C::NI>([&](auto ci_) {
+                                    constexpr int ci = decltype(ci_)::value;
+                                    constexpr double wi = sph_coef(LI, I, ci);
+                                    if constexpr (wi != 0.0) {
+                                        double vj = 0.0;
+                                        static_for<0, C::NJ>([&](auto cj_) {
+                                            constexpr int cj = decltype(cj_)::value;
+                                            constexpr double wj = sph_coef(LJ, J, cj);
+                                            if constexpr (wj != 0.0) vj = fma(wj, acc[ci * C::NJ + cj][c], vj);
+                                        });
+                                        v = fma(wi, vj, v);
+                                    }
+                                });
+                                if (valid) {
+                                    const size_t row = ((size_t)sp_local * C::NIJS + I * nsph(LJ) + J) * C::NKO + ko;
+                                    out[obase + row * n_aux + a_local] = v;
+                                    wsum += v;
                                 }
                             });
-                            const size_t row = ((size_t)sp * nsph(LI) * nsph(LJ) + I * nsph(LJ) + J) * C::NKO + ko;
-                            out[row * n_ket + a] = v;
                         });
-                    });
-                }
-            });
+                    }
+                });
+            }
+        });
+        if (map.checksum) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+            if (lane == 0) atomicAdd(map.checksum + m, wsum);
         }
-    });
+    }
 }
 
+// Occupancy-sized persistent grid for one class.
 template <int LI, int LJ, int LK>
-static int launch_one(const double* boys_table, const BraTable& bra, const KetTable& ket, double omega, double* out,
-                      cudaStream_t s) {
+static int launch_one(const double* boys_table, const BraTable& bra, const KetTable& ket, const BatchMap& map,
+                      int total_items, double omega, double* out, int* counter, cudaStream_t s) {
     using C = Fast3c<LI, LJ, LK>;
-    if (bra.n_group == 0 || ket.n_group == 0) return 0;
-    const int n_tiles = (ket.n_group + 31) / 32;
-    const long long blocks = (long long)bra.n_group * n_tiles;
-    if (blocks > 0x7fffffffLL) return 3;
-    k3c_fast<LI, LJ, LK><<<(unsigned)blocks, C::THREADS, 0, s>>>(boys_table, bra, ket, n_tiles, omega, out);
+    if (total_items <= 0) return 0;
+    static int max_blocks = 0;
+    if (max_blocks == 0) {
+        int per_sm = 0, dev = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3c_fast<LI, LJ, LK>, C::THREADS, 0) != cudaSuccess)
+            return 2;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        max_blocks = (per_sm < 1 ? 1 : per_sm) * sms;
+    }
+    const int blocks = total_items < max_blocks ? total_items : max_blocks;
+    k3c_fast<LI, LJ, LK><<<blocks, C::THREADS, 0, s>>>(boys_table, bra, ket, map, omega, out, counter, total_items);
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+template <int LI, int LJ>
+static int launch_e_table(const BraTable& bra, double* prim_E, cudaStream_t s) {
+    if (bra.n_group == 0) return 0;
+    e_table_kernel<LI, LJ><<<(bra.n_group + 127) / 128, 128, 0, s>>>(bra, prim_E);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 

@@ -1,18 +1,24 @@
-// Fast (mu nu|P) instances for (l_i, l_j) = (1, 2), l_k = 0..4.
+// Fast (mu nu|P) instances for (l_i, l_j) = (1, 2), l_k = 0..4, and the
+// E-table kernel of this pair class.
 #include "k3c_fast.cuh"
 
 namespace eip {
 
-int launch_fast3c_12(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket, double omega,
-                        double* out, cudaStream_t s) {
+int launch_fast3c_12(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket,
+                        const BatchMap& map, int total_items, double omega, double* out, int* counter,
+                        cudaStream_t s) {
     switch (lk) {
-        case 0: return launch_one<1, 2, 0>(boys_table, bra, ket, omega, out, s);
-        case 1: return launch_one<1, 2, 1>(boys_table, bra, ket, omega, out, s);
-        case 2: return launch_one<1, 2, 2>(boys_table, bra, ket, omega, out, s);
-        case 3: return launch_one<1, 2, 3>(boys_table, bra, ket, omega, out, s);
-        case 4: return launch_one<1, 2, 4>(boys_table, bra, ket, omega, out, s);
+        case 0: return launch_one<1, 2, 0>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 1: return launch_one<1, 2, 1>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 2: return launch_one<1, 2, 2>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 3: return launch_one<1, 2, 3>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 4: return launch_one<1, 2, 4>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
     }
     return 1;
+}
+
+int launch_e_table_12(const BraTable& bra, double* prim_E, cudaStream_t s) {
+    return launch_e_table<1, 2>(bra, prim_E, s);
 }
 
 }  // namespace eip

@@ -7,8 +7,9 @@ real chemistry with the shapes, sizes and value ranges the workloads name:
   H-O-H 104.5 deg), uniform random centres in a cube, uniform random
   orientation (unit quaternion), O-O distance >= 2.6 A by rejection.
 * ``organic_molecule(n_atom, seed)`` -- H/C/N/O (0.5/0.3/0.1/0.1) grown by
-  random bonded placement: X-H 1.09 A, heavy-heavy U[1.40, 1.54] A, every
-  non-bonded distance >= 2.0 A.
+  random bonded placement within valences (C 4, N 3, O 2): X-H 1.09 A,
+  heavy-heavy U[1.40, 1.54] A, non-bonded distances >= 2.0 A (geminal 1-3
+  pairs >= 1.6 A).
 * ``orbital_basis_text(elements, seed)`` -- Gaussian-format text; O/C/N get
   3s2p1d and H 2s1p.  Every shell draws 1-6 distinct exponents (uniform count)
   from an even-tempered ladder of ratio 3.0 starting at 0.12 and capped at
@@ -68,31 +69,72 @@ def water_cluster(n_water: int, box_angstrom: float, seed: int = 0, min_oo: floa
     return Molecule(elements=elements, geometry=np.array(xyz) * angstrom_to_bohr, spherical_basis=True)
 
 
+_VALENCE = {"C": 4, "N": 3, "O": 2}
+
+
+def _place(rng, xyz, neighbours, parent, bond):
+    """Random direction around `parent` keeping non-bonded distances >= 2.0 A
+    (>= 1.6 A to the parent's other neighbours); relaxes both floors by 10 %
+    after every 200 failed directions, so it always terminates."""
+    floor_nb, floor_gem = 2.0, 1.6
+    for _ in range(50):
+        for _ in range(200):
+            v = rng.normal(size=3)
+            pos = xyz[parent] + bond * v / np.linalg.norm(v)
+            gem = set(neighbours[parent])
+            if all(k == parent or np.linalg.norm(pos - xyz[k]) >= (floor_gem if k in gem else floor_nb)
+                   for k in range(len(xyz))):
+                return pos
+        floor_nb *= 0.9
+        floor_gem *= 0.9
+    return pos
+
+
 def organic_molecule(n_atom: int, seed: int = 0) -> Molecule:
+    """Grow a molecule by random bonded placement (see module docstring).
+
+    Composition is drawn first (H/C/N/O 0.5/0.3/0.1/0.1, first atom heavy);
+    hydrogens beyond the skeleton's free valences (C 4, N 3, O 2) become carbon.
+    The heavy-atom tree is grown first, then hydrogens fill free valences.
+    """
+    if n_atom < 1:
+        raise ValueError("n_atom must be >= 1")
     rng = np.random.default_rng(seed)
     symbols = np.array(["H", "C", "N", "O"])
     probs = np.array([0.5, 0.3, 0.1, 0.1])
     heavy_probs = probs[1:] / probs[1:].sum()
-    elements = [str(rng.choice(symbols[1:], p=heavy_probs))]
-    xyz = [np.zeros(3)]
-    while len(elements) < n_atom:
-        el = str(rng.choice(symbols, p=probs))
-        heavy = [i for i, e in enumerate(elements) if e != "H"]
-        placed = False
-        for _ in range(200):
-            parent = heavy[rng.integers(len(heavy))]
-            bond = 1.09 if (el == "H") else rng.uniform(1.40, 1.54)
-            v = rng.normal(size=3)
-            pos = xyz[parent] + bond * v / np.linalg.norm(v)
-            ok = all(np.linalg.norm(pos - xyz[k]) >= 2.0 for k in range(len(xyz)) if k != parent)
-            if ok:
-                elements.append(el)
-                xyz.append(pos)
-                placed = True
-                break
-        if not placed:
-            # Crowded: fall back to a heavy atom so the skeleton can grow outwards.
-            continue
+    elems = [str(rng.choice(symbols[1:], p=heavy_probs))] + [str(rng.choice(symbols, p=probs))
+                                                               for _ in range(n_atom - 1)]
+    while True:
+        heavy = [e for e in elems if e != "H"]
+        capacity = sum(_VALENCE[e] for e in heavy) - 2 * (len(heavy) - 1)
+        n_h = len(elems) - len(heavy)
+        if n_h <= capacity:
+            break
+        elems[elems.index("H")] = "C"
+    heavy = [e for e in elems if e != "H"]
+    elements, xyz, neighbours, free = [heavy[0]], [np.zeros(3)], [[]], [_VALENCE[heavy[0]]]
+    for el in heavy[1:]:
+        # keep a free valence on the tree for every heavy atom still to come
+        cand = [i for i in range(len(elements)) if free[i] >= 2] or [i for i in range(len(elements)) if free[i] >= 1]
+        parent = cand[rng.integers(len(cand))]
+        pos = _place(rng, xyz, neighbours, parent, rng.uniform(1.40, 1.54))
+        elements.append(el)
+        xyz.append(pos)
+        neighbours.append([parent])
+        neighbours[parent].append(len(xyz) - 1)
+        free.append(_VALENCE[el] - 1)
+        free[parent] -= 1
+    for _ in range(len(elems) - len(heavy)):
+        cand = [i for i in range(len(elements)) if elements[i] != "H" and free[i] >= 1]
+        parent = cand[rng.integers(len(cand))]
+        pos = _place(rng, xyz, neighbours, parent, 1.09)
+        elements.append("H")
+        xyz.append(pos)
+        neighbours.append([parent])
+        neighbours[parent].append(len(xyz) - 1)
+        free.append(0)
+        free[parent] -= 1
     return Molecule(elements=elements, geometry=np.array(xyz) * angstrom_to_bohr, spherical_basis=True)
 
 

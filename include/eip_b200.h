@@ -82,6 +82,56 @@ float eip_last_kernel_ms(void);
 /* Device Boys function: F[i*(L+1)+m] = F_m(T[i]), m = 0..L <= 21 (host buffers). */
 int eip_boys(int L, const double* T, int n, double* F);
 
+/* FMA-throughput microbenchmark on the current device (fp64 != 0: double,
+ * else float), best of 5 runs, in TFLOP/s: the denominators of the rooflines. */
+int eip_measure_fma_peak(int fp64, double* tflops);
+
+/* ---- batched (mu nu|P) over many molecules (no counterpart in the reference) --
+ *
+ * Usage: create -> add_pairs / add_aux per molecule and class (host arrays in
+ * the reference ABI's formats; may be called repeatedly) -> build (groups the
+ * primitives, uploads device-resident tables) -> alloc_output or bind_output
+ * -> run (one CUDA-graph launch: every class kernel of every molecule) -> sync.
+ * Output: one packed block per (molecule, class) at eip_batch_block()'s
+ * offset, layout [pair shell][I][J][K][aux shell] with spherical components
+ * I, J, K (Cartesian when spherical is false); pair shells are ordered by
+ * (i_ao_start, j_ao_start), auxiliary shells by aux start.  Each element is
+ * written once; nothing is accumulated.  Returns: 0 ok, 1 unsupported class,
+ * 2 failure (eip_batch_error). */
+typedef struct eip_batch eip_batch;
+
+eip_batch* eip_batch_create(int n_molecules, bool spherical, double omega);
+int eip_batch_add_pairs(eip_batch* batch, int molecule, int i_L, int j_L, const double* pair_P_p,
+                        const double* pair_A_a, const double* pair_B_b, const double* pair_coefficient,
+                        const int* pair_i_ao_start, const int* pair_j_ao_start, int n_pair);
+int eip_batch_add_aux(eip_batch* batch, int molecule, int k_L, const double* aux_A_a,
+                      const double* aux_coefficient, const int* aux_i_aux_start, int n_primitive);
+int eip_batch_build(eip_batch* batch);
+long long eip_batch_output_elems(eip_batch* batch);
+int eip_batch_block(eip_batch* batch, int molecule, int i_L, int j_L, int k_L, long long* offset,
+                    int* n_pair_shells, int* n_aux_shells);
+int eip_batch_alloc_output(eip_batch* batch);
+int eip_batch_bind_output(eip_batch* batch, double* device_output);
+double* eip_batch_output_device(eip_batch* batch);
+/* checksum != 0: also accumulate, per molecule, the sum of its written values. */
+int eip_batch_run(eip_batch* batch, int checksum);
+/* Launch the kernels of one (i_L, j_L | k_L) class alone, on the batch stream,
+ * outside the graph (per-kernel timing); returns 1 if the class is absent. */
+int eip_batch_run_class(eip_batch* batch, int i_L, int j_L, int k_L);
+int eip_batch_sync(eip_batch* batch);
+/* 0 if every class kernel of the last run passed its self-checks, 3 if one
+ * recorded an inconsistency (eip_batch_error names it). */
+int eip_batch_status(eip_batch* batch);
+/* Re-copy every input table from the batch's pinned host copy to the device. */
+int eip_batch_upload(eip_batch* batch);
+long long eip_batch_table_bytes(eip_batch* batch);
+unsigned long long eip_batch_launches_per_run(eip_batch* batch);
+int eip_batch_checksums(eip_batch* batch, double* host_checksums);
+int eip_batch_copy_output(eip_batch* batch, long long offset, long long count, double* host);
+void* eip_batch_stream(eip_batch* batch);
+const char* eip_batch_error(eip_batch* batch);
+void eip_batch_destroy(eip_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,3 +58,18 @@ def test_pair_tables_bit_identical(name):
         for k, ref in c.aux_data.items():
             for f in ("A_a", "coefficient", "i_ao_start"):
                 assert np.array_equal(getattr(aux[k], f), getattr(ref, f)), (k, f)
+
+
+def test_synthetic_generators_terminate_and_respect_geometry():
+    syn = importlib.import_module("electron-integral-playground_b200.synthetic")
+    for seed in range(40):
+        for n in (1, 3, 7, 25):
+            m = syn.organic_molecule(n, seed)
+            assert len(m.elements) == n
+            if n > 1:
+                d = np.linalg.norm(m.geometry[:, None] - m.geometry[None], axis=-1) * 0.52917721054482
+                assert np.min(d[np.triu_indices(n, 1)]) > 0.9
+    w = syn.water_cluster(10, 9.0, 0)
+    o = w.geometry[0::3] * 0.52917721054482
+    d = np.linalg.norm(o[:, None] - o[None], axis=-1)
+    assert np.min(d[np.triu_indices(10, 1)]) >= 2.6
