@@ -82,6 +82,29 @@ float eip_last_kernel_ms(void);
 /* Device Boys function: F[i*(L+1)+m] = F_m(T[i]), m = 0..L <= 21 (host buffers). */
 int eip_boys(int L, const double* T, int n, double* F);
 
+/* (mu nu|P) of one class like three_center(), for callers that cannot let the
+ * library allocate device memory (a framework's memory pool or a program that
+ * reserves device memory up front owns it; an allocation could stall or fail
+ * mid-run or synchronise the device).  No counterpart in the reference.
+ * Every pointer is a DEVICE pointer; J3c_matrix[n_aux][n_ao][n_ao] is
+ * accumulated (+=) asynchronously on `stream` (a cudaStream_t, 0 = default).
+ * Nothing is allocated: working memory is one fixed 16 MiB device array per
+ * GPU, held from module load until exit.  Limit: a call needing more of it
+ * (roughly n_pair_ij x n_aux_primitive_k primitive triplets times the class's
+ * Cartesian plus output block) returns 4 with a message on stderr and launches
+ * nothing; at most 65535 auxiliary primitives.  All calls share the array:
+ * calls whose kernels overlap on the GPU race, so order them (one stream).
+ * The first call on each device (with it current) looks up the array's address
+ * and uploads the constant tables; make it before any stream capture.
+ * Returns 0, 1 (unsupported class), 2 (CUDA failure) or 4 (too large). */
+int eip_three_center_noalloc(const int i_L, const int j_L, const int k_L,
+                             const double* pair_P_p, const double* pair_A_a, const double* pair_B_b,
+                             const double* pair_coefficient, const int* pair_i_ao_start,
+                             const int* pair_j_ao_start, const int n_pair_ij, const double* aux_A_a,
+                             const double* aux_coefficient, const int* aux_i_aux_start,
+                             const int n_aux_primitive_k, double* J3c_matrix, const int n_ao, const int n_aux,
+                             const bool spherical, const double omega, void* stream);
+
 /* FMA-throughput microbenchmark on the current device (fp64 != 0: double,
  * else float), best of 5 runs, in TFLOP/s: the denominators of the rooflines. */
 int eip_measure_fma_peak(int fp64, double* tflops);
