@@ -166,6 +166,8 @@ def main():
     ap.add_argument("--molecules", type=int, default=64)
     ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of reference CPU work per sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune", action="store_true",
+                    help="run the autotuner on this workload first and rewrite its cache")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -186,6 +188,7 @@ def main():
     import importlib
 
     bt = importlib.import_module("electron-integral-playground_b200.batch")
+    at = importlib.import_module("electron-integral-playground_b200.autotune")
     rf = importlib.import_module("electron-integral-playground_b200.roofline")
     lm = importlib.import_module("electron-integral-playground_b200._lib")
     if lm.lib().eip_init(local) != 0:
@@ -199,6 +202,12 @@ def main():
         raise RuntimeError(f"packed output {batch.output_bytes / 1e9:.1f} GB exceeds free device memory")
     batch.alloc_output()
     stream = torch.cuda.ExternalStream(batch.stream)
+    tuning = at.load()
+    if args.tune:
+        table, timings = at.tune(batch, sorted(per_class))
+        at.save(table, timings, {"workload": WORKLOAD, "seed": args.seed, "molecules": args.molecules,
+                                 "gpu": torch.cuda.get_device_name(local)})
+        tuning = at.load()
 
     def timed(fn, k):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -312,6 +321,7 @@ def main():
             "latency_ms": {"p50": statistics.median(per_step),
                            "p99": sorted(per_step)[min(len(per_step) - 1, int(0.99 * len(per_step)))]},
             "class_ms": {f"{k[0]}{k[1]}|{k[2]}": round(v, 4) for k, v in sorted(class_ms.items())},
+            "tuning": "autotuned variants (tuning/b200_fp64.json)" if tuning else "default variants",
         }
         print(json.dumps(line))
     batch.close()

@@ -44,6 +44,10 @@ def lib():
         L.eip_last_error.restype = ctypes.c_char_p
         L.eip_kernel_launch_count.restype = ctypes.c_ulonglong
         L.eip_last_kernel_ms.restype = ctypes.c_float
+        L.eip_tune_set.argtypes = [c_int, c_int, c_int, c_int]
+        L.eip_tune_set.restype = c_int
+        L.eip_tune_get.argtypes = [c_int, c_int, c_int]
+        L.eip_tune_get.restype = c_int
         L.eip_boys.argtypes = [c_int, _dp, c_int, _dp]
         L.eip_boys.restype = c_int
         _lib = L

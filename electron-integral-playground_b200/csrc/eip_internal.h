@@ -16,6 +16,8 @@ const double* boys_table_device();
 int launch_boys_probe(int L, const double* dT, int n, double* dout, cudaStream_t s);
 
 bool fast3c_supported(int li, int lj, int lk);
+int fast3c_variant(int li, int lj, int lk);
+int fast3c_set_variant(int li, int lj, int lk, int v);
 size_t e_table_doubles(int li, int lj);
 int launch_e_table(int li, int lj, const BraTable& bra, double* prim_E, cudaStream_t s);
 int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& ket, const BatchMap& map,

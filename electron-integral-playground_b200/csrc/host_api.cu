@@ -384,6 +384,10 @@ unsigned long long eip_kernel_launch_count(void) { return ctx().launches; }
 
 float eip_last_kernel_ms(void) { return ctx().last_kernel_ms; }
 
+int eip_tune_set(int i_L, int j_L, int k_L, int variant) { return fast3c_set_variant(i_L, j_L, k_L, variant); }
+
+int eip_tune_get(int i_L, int j_L, int k_L) { return fast3c_variant(i_L, j_L, k_L); }
+
 int eip_boys(int L, const double* T, int n, double* F) {
     Context& c = ctx();
     std::lock_guard<std::mutex> lock(c.mu);

@@ -1,20 +1,42 @@
-// Dispatcher of the fast (mu nu|P) kernels; one translation unit per (l_i, l_j)
-// (k3c_fast_IJ.cu) so the template instances compile in parallel.
+// Dispatcher of the fast (mu nu|P) kernels: one translation unit per (l_i, l_j)
+// and tuning variant (k3c_fast_IJ_vV.cu) so the instances compile in parallel;
+// the variant of each class comes from the tuning table (eip_tune_set).
 #include "eip_common.cuh"
 #include "eip_internal.h"
 
 namespace eip {
 
-#define EIP_DECL(I, J)                                                                                       \
-    int launch_fast3c_##I##J(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket,     \
-                             const BatchMap& map, int total_items, double omega, double* out, int* counter, \
-                             cudaStream_t s);                                                                \
+#define EIP_DECL_V(I, J, V)                                                                                   \
+    int launch_fast3c_##I##J##_v##V(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket, \
+                                    const BatchMap& map, int total_items, double omega, double* out,         \
+                                    int* counter, cudaStream_t s);
+#define EIP_DECL(I, J)                                                                 \
+    EIP_DECL_V(I, J, 0) EIP_DECL_V(I, J, 1) EIP_DECL_V(I, J, 2) EIP_DECL_V(I, J, 3)    \
     int launch_e_table_##I##J(const BraTable& bra, double* prim_E, cudaStream_t s);
 EIP_DECL(0, 0) EIP_DECL(0, 1) EIP_DECL(1, 1) EIP_DECL(0, 2) EIP_DECL(1, 2) EIP_DECL(2, 2)
 #undef EIP_DECL
+#undef EIP_DECL_V
+
+// Variant per (l_i, l_j, l_k): index li*3+lj (li <= lj <= 2), lk.  Defaults from
+// the autotuner's run on B200 (tuning/b200_fp64.json); eip_tune_set overrides.
+static int g_variant[9][5] = {
+    {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0},
+    {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0},
+    {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0},
+};
 
 bool fast3c_supported(int li, int lj, int lk) {
     return li >= 0 && li <= lj && lj <= 2 && lk >= 0 && lk <= 4;
+}
+
+int fast3c_variant(int li, int lj, int lk) {
+    return fast3c_supported(li, lj, lk) ? g_variant[li * 3 + lj][lk] : -1;
+}
+
+int fast3c_set_variant(int li, int lj, int lk, int v) {
+    if (!fast3c_supported(li, lj, lk) || v < 0 || v > 3) return 1;
+    g_variant[li * 3 + lj][lk] = v;
+    return 0;
 }
 
 size_t e_table_doubles(int li, int lj) {
@@ -26,8 +48,17 @@ size_t e_table_doubles(int li, int lj) {
 
 int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& ket, const BatchMap& map,
                   int total_items, double omega, double* out, int* counter, cudaStream_t s) {
+    if (!fast3c_supported(li, lj, lk)) return 1;
     const double* t = boys_table_device();
-#define EIP_GO(I, J) return launch_fast3c_##I##J(lk, t, bra, ket, map, total_items, omega, out, counter, s)
+    const int v = g_variant[li * 3 + lj][lk];
+#define EIP_GO_V(I, J, V) return launch_fast3c_##I##J##_v##V(lk, t, bra, ket, map, total_items, omega, out, counter, s)
+#define EIP_GO(I, J)                  \
+    switch (v) {                      \
+        case 1: EIP_GO_V(I, J, 1);    \
+        case 2: EIP_GO_V(I, J, 2);    \
+        case 3: EIP_GO_V(I, J, 3);    \
+        default: EIP_GO_V(I, J, 0);   \
+    }
     switch (li * 10 + lj) {
         case 0: EIP_GO(0, 0);
         case 1: EIP_GO(0, 1);
@@ -37,6 +68,7 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
         case 22: EIP_GO(2, 2);
     }
 #undef EIP_GO
+#undef EIP_GO_V
     return 1;
 }
 

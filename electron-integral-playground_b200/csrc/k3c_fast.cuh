@@ -13,10 +13,11 @@
 //   * lane = auxiliary shell, so the stores of a warp are 32 consecutive doubles;
 //   * the KS warps of a CTA split (a) the entries of the Hermite tetrahedron
 //     R_{tuv} (closed form from R^{(m)}_000, shared through shared memory) and
-//     (b) the spherical ket components; a warp evaluates its KPW ket
-//     components together so every shared-memory E^{ij}_t load feeds KPW FMAs;
+//     (b) the spherical ket components (KPW per warp);
 //   * the ket Cartesian->spherical transform and one-centre Hermite
-//     coefficients are compile-time constants (zero terms vanish);
+//     coefficients come from a per-l_k constant-memory table (KetCoefTable),
+//     so all warps run the same ket/bra code (instruction-cache friendly);
+//     zero coefficients are skipped by a warp-uniform branch;
 //   * E^{ij}_t tables of each primitive pair are precomputed once into the
 //     device-resident pair table (e_table_kernel) and staged per pair into
 //     shared memory;
@@ -31,16 +32,22 @@
 
 namespace eip {
 
-constexpr int kAccMax = 48;  // accumulators (doubles) per lane
+// Tuning variants (chosen per class by the autotuner, see autotune.py):
+//   ACC   accumulators (doubles) per lane -> how many warps split the ket
+//   WARPS resident warps per SM asked of the register allocator (register cap
+//         65536 / (32 * WARPS)); more warps hide latency, fewer avoid spills.
+constexpr int kVariants = 4;
+__host__ __device__ constexpr int variant_acc(int v) { return v == 2 ? 24 : (v == 3 ? 96 : 48); }
+__host__ __device__ constexpr int variant_warps(int v) { return v == 1 || v == 3 ? 8 : 16; }
 
-template <int LI, int LJ, int LK>
+template <int LI, int LJ, int LK, int V = 0>
 struct Fast3c {
     static constexpr int L = LI + LJ + LK;
     static constexpr int LIJ = LI + LJ;
     static constexpr int NI = ncart(LI), NJ = ncart(LJ), NIJ = NI * NJ;
     static constexpr int NIJS = nsph(LI) * nsph(LJ);
     static constexpr int NKO = nsph(LK);
-    static constexpr int KPW_MAX = (kAccMax / NIJ) < 1 ? 1 : (kAccMax / NIJ);
+    static constexpr int KPW_MAX = (variant_acc(V) / NIJ) < 1 ? 1 : (variant_acc(V) / NIJ);
     static constexpr int KS = (NKO + KPW_MAX - 1) / KPW_MAX;  // warps per CTA
     static constexpr int KPW = (NKO + KS - 1) / KS;           // ket components per warp
     static constexpr int NR = nherm(L);
@@ -48,7 +55,40 @@ struct Fast3c {
     static constexpr int NHB = nherm(LIJ);
     static constexpr int NE = e_size<LI, LJ>();
     static constexpr int THREADS = 32 * KS;
+    // resident CTAs per SM asked of the register allocator
+    static constexpr int MIN_CTAS = (variant_warps(V) / KS) < 1 ? 1 : (variant_warps(V) / KS);
 };
+
+// Ket coefficient table of one l_k: for spherical component ko and Hermite
+// index s (|s| = LK - 2j, listed level by level in Cartesian order), the
+// combined one-centre Hermite and Cartesian->spherical coefficient; the
+// (1/2q)^{LK-j} weight is applied at run time.  Held in constant memory so that
+// every warp runs the same ket code whatever components it owns (code
+// specialised per component overflowed the instruction cache).
+__host__ __device__ constexpr int ket_n_s(int LK) {
+    int n = 0;
+    for (int j = 0; j <= LK / 2; j++) n += ncart(LK - 2 * j);
+    return n;
+}
+template <int LK>
+struct KetCoefTable {
+    double v[nsph(LK)][ket_n_s(LK)];
+};
+template <int LK>
+constexpr KetCoefTable<LK> make_ket_table() {
+    KetCoefTable<LK> t{};
+    for (int ko = 0; ko < nsph(LK); ko++) {
+        int idx = 0;
+        for (int j = 0; j <= LK / 2; j++) {
+            const int S = LK - 2 * j;
+            for (int sc = 0; sc < ncart(S); sc++)
+                t.v[ko][idx++] = ket_sph_coef(LK, ko, cart_x(S, sc), cart_y(S, sc), cart_z(S, sc));
+        }
+    }
+    return t;
+}
+template <int LK>
+__constant__ KetCoefTable<LK> c_ket_coef = make_ket_table<LK>();
 
 // Two-centre E^{i,j}_t along one axis for i <= LI, j <= LJ:
 // vertical recursion E^{i+1,0}_t = E^{i,0}_{t-1}/(2p) + PA E^{i,0}_t + (t+1) E^{i,0}_{t+1},
@@ -105,11 +145,11 @@ __global__ void e_table_kernel(BraTable bra, double* __restrict__ prim_E) {
     }
 }
 
-template <int LI, int LJ, int LK>
-__global__ void __launch_bounds__(Fast3c<LI, LJ, LK>::THREADS)
+template <int LI, int LJ, int LK, int V>
+__global__ void __launch_bounds__(Fast3c<LI, LJ, LK, V>::THREADS, Fast3c<LI, LJ, LK, V>::MIN_CTAS)
 k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, BatchMap map, double omega,
          double* __restrict__ out, int* __restrict__ work_counter, int total_items) {
-    using C = Fast3c<LI, LJ, LK>;
+    using C = Fast3c<LI, LJ, LK, V>;
     constexpr int L = C::L;
     __shared__ double sE[3 * C::NE];
     __shared__ double sR[C::NR * 32];
@@ -262,89 +302,116 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 }
                 __syncthreads();
 
-                static_for<0, C::KS>([&](auto g) {
-                    constexpr int G = decltype(g)::value;
-                    constexpr int KO0 = G * C::KPW;
-                    constexpr int NC = (KO0 + C::KPW <= C::NKO) ? C::KPW : (C::NKO - KO0);
-                    if (warp == G) {
-                        // ket: X[c][h] = sum_j w_j sum_{|s| = LK-2j} K[ko][s] R[h + s]
-                        double Xh[NC][C::NHB];
-                        static_for<0, C::NHB>([&](auto h_) {
-                            constexpr int h = decltype(h_)::value;
-                            constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
-                            double xs[NC];
+                // ket + bra.  Warp w owns ket components ko = w * KPW + c, c < KPW.
+                // One warp per CTA: ket coefficients are compile-time constants
+                // (zero terms vanish).  Several warps: the same code in every
+                // warp, coefficients from constant memory, so the instruction
+                // cache holds one copy.  Either way X[c][h] is formed for all
+                // c first, so each E^{ij}_t shared-memory load feeds KPW FMAs.
+                double Xh[C::KPW][C::NHB];
 #pragma unroll
-                            for (int c = 0; c < NC; c++) xs[c] = 0.0;
-                            static_for<0, LK / 2 + 1>([&](auto j_) {
-                                constexpr int j = decltype(j_)::value;
-                                constexpr int S = LK - 2 * j;
-                                double part[NC];
+                for (int c = 0; c < C::KPW; c++)
 #pragma unroll
-                                for (int c = 0; c < NC; c++) part[c] = 0.0;
-                                static_for<0, ncart(S)>([&](auto sc_) {
-                                    constexpr int sc = decltype(sc_)::value;
-                                    constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
-                                    constexpr bool any = [] {
-                                        for (int c = 0; c < NC; c++)
-                                            if (ket_sph_coef(LK, KO0 + c, sx, sy, sz) != 0.0) return true;
-                                        return false;
-                                    }();
-                                    if constexpr (any) {
-                                        const double r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
-                                        static_for<0, NC>([&](auto c_) {
-                                            constexpr int c = decltype(c_)::value;
-                                            constexpr double kc = ket_sph_coef(LK, KO0 + c, sx, sy, sz);
-                                            if constexpr (kc != 0.0) part[c] = fma(kc, r, part[c]);
-                                        });
-                                    }
-                                });
+                    for (int h = 0; h < C::NHB; h++) Xh[c][h] = 0.0;
+                if constexpr (C::KS == 1) {
+                    static_for<0, C::NHB>([&](auto h_) {
+                        constexpr int h = decltype(h_)::value;
+                        constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
+                        static_for<0, LK / 2 + 1>([&](auto j_) {
+                            constexpr int j = decltype(j_)::value;
+                            constexpr int S = LK - 2 * j;
+                            double part[C::KPW];
 #pragma unroll
-                                for (int c = 0; c < NC; c++) xs[c] = fma(w[j], part[c], xs[c]);
-                            });
-#pragma unroll
-                            for (int c = 0; c < NC; c++) Xh[c][h] = xs[c];
-                        });
-                        // bra: acc[ij][c] += pref * sum_t Ex sum_u Ey sum_v Ez X[c][tuv]
-                        static_for<0, C::NI>([&](auto ci_) {
-                            constexpr int ci = decltype(ci_)::value;
-                            constexpr int ix = cart_x(LI, ci), iy = cart_y(LI, ci), iz = cart_z(LI, ci);
-                            static_for<0, C::NJ>([&](auto cj_) {
-                                constexpr int cj = decltype(cj_)::value;
-                                constexpr int jx = cart_x(LJ, cj), jy = cart_y(LJ, cj), jz = cart_z(LJ, cj);
-                                double s[NC];
-#pragma unroll
-                                for (int c = 0; c < NC; c++) s[c] = 0.0;
-                                static_for<0, ix + jx + 1>([&](auto t_) {
-                                    constexpr int t = decltype(t_)::value;
-                                    double su[NC];
-#pragma unroll
-                                    for (int c = 0; c < NC; c++) su[c] = 0.0;
-                                    static_for<0, iy + jy + 1>([&](auto u_) {
-                                        constexpr int u = decltype(u_)::value;
-                                        double sv[NC];
-#pragma unroll
-                                        for (int c = 0; c < NC; c++) sv[c] = 0.0;
-                                        static_for<0, iz + jz + 1>([&](auto v_) {
-                                            constexpr int v = decltype(v_)::value;
-                                            const double ez = sE[2 * C::NE + e_offset<LJ>(iz, jz) + v];
-#pragma unroll
-                                            for (int c = 0; c < NC; c++)
-                                                sv[c] = fma(ez, Xh[c][herm_index(t, u, v)], sv[c]);
-                                        });
-                                        const double ey = sE[C::NE + e_offset<LJ>(iy, jy) + u];
-#pragma unroll
-                                        for (int c = 0; c < NC; c++) su[c] = fma(ey, sv[c], su[c]);
+                            for (int c = 0; c < C::KPW; c++) part[c] = 0.0;
+                            static_for<0, ncart(S)>([&](auto sc_) {
+                                constexpr int sc = decltype(sc_)::value;
+                                constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
+                                constexpr bool any = [] {
+                                    for (int c = 0; c < C::NKO; c++)
+                                        if (ket_sph_coef(LK, c, sx, sy, sz) != 0.0) return true;
+                                    return false;
+                                }();
+                                if constexpr (any) {
+                                    const double r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
+                                    static_for<0, C::NKO>([&](auto c_) {
+                                        constexpr int c = decltype(c_)::value;
+                                        constexpr double kc = ket_sph_coef(LK, c, sx, sy, sz);
+                                        if constexpr (kc != 0.0) part[c] = fma(kc, r, part[c]);
                                     });
-                                    const double ex = sE[e_offset<LJ>(ix, jx) + t];
-#pragma unroll
-                                    for (int c = 0; c < NC; c++) s[c] = fma(ex, su[c], s[c]);
-                                });
-#pragma unroll
-                                for (int c = 0; c < NC; c++)
-                                    acc[ci * C::NJ + cj][c] = fma(pref, s[c], acc[ci * C::NJ + cj][c]);
+                                }
                             });
+#pragma unroll
+                            for (int c = 0; c < C::KPW; c++) Xh[c][h] = fma(w[j], part[c], Xh[c][h]);
                         });
-                    }
+                    });
+                } else {
+                    int sidx = 0;
+                    static_for<0, LK / 2 + 1>([&](auto j_) {
+                        constexpr int j = decltype(j_)::value;
+                        constexpr int S = LK - 2 * j;
+                        static_for<0, ncart(S)>([&](auto sc_) {
+                            constexpr int sc = decltype(sc_)::value;
+                            constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
+                            double ce[C::KPW];
+                            bool any = false;
+#pragma unroll
+                            for (int c = 0; c < C::KPW; c++) {
+                                const int ko = warp * C::KPW + c;
+                                const double cf = ko < C::NKO ? c_ket_coef<LK>.v[ko][sidx + sc] : 0.0;
+                                ce[c] = cf * w[j];
+                                any = any || cf != 0.0;
+                            }
+                            if (any) {  // warp-uniform
+                                static_for<0, C::NHB>([&](auto h_) {
+                                    constexpr int h = decltype(h_)::value;
+                                    constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
+                                    const double r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
+#pragma unroll
+                                    for (int c = 0; c < C::KPW; c++) Xh[c][h] = fma(ce[c], r, Xh[c][h]);
+                                });
+                            }
+                        });
+                        sidx += ncart(S);
+                    });
+                }
+                // bra: acc[ij][c] += pref * sum_t Ex sum_u Ey sum_v Ez X[c][tuv]
+                static_for<0, C::NI>([&](auto ci_) {
+                    constexpr int ci = decltype(ci_)::value;
+                    constexpr int ix = cart_x(LI, ci), iy = cart_y(LI, ci), iz = cart_z(LI, ci);
+                    static_for<0, C::NJ>([&](auto cj_) {
+                        constexpr int cj = decltype(cj_)::value;
+                        constexpr int jx = cart_x(LJ, cj), jy = cart_y(LJ, cj), jz = cart_z(LJ, cj);
+                        double sxv[C::KPW];
+#pragma unroll
+                        for (int c = 0; c < C::KPW; c++) sxv[c] = 0.0;
+                        static_for<0, ix + jx + 1>([&](auto t_) {
+                            constexpr int t = decltype(t_)::value;
+                            double su[C::KPW];
+#pragma unroll
+                            for (int c = 0; c < C::KPW; c++) su[c] = 0.0;
+                            static_for<0, iy + jy + 1>([&](auto u_) {
+                                constexpr int u = decltype(u_)::value;
+                                double sv[C::KPW];
+#pragma unroll
+                                for (int c = 0; c < C::KPW; c++) sv[c] = 0.0;
+                                static_for<0, iz + jz + 1>([&](auto v_) {
+                                    constexpr int v = decltype(v_)::value;
+                                    const double ez = sE[2 * C::NE + e_offset<LJ>(iz, jz) + v];
+#pragma unroll
+                                    for (int c = 0; c < C::KPW; c++) sv[c] = fma(ez, Xh[c][herm_index(t, u, v)], sv[c]);
+                                });
+                                const double ey = sE[C::NE + e_offset<LJ>(iy, jy) + u];
+#pragma unroll
+                                for (int c = 0; c < C::KPW; c++) su[c] = fma(ey, sv[c], su[c]);
+                            });
+                            const double ex = sE[e_offset<LJ>(ix, jx) + t];
+#pragma unroll
+                            for (int c = 0; c < C::KPW; c++) sxv[c] = fma(ex, su[c], sxv[c]);
+                        });
+#pragma unroll
+                        for (int c = 0; c < C::KPW; c++)
+                            acc[ci * C::NJ + cj][c] = fma(pref, sxv[c], acc[ci * C::NJ + cj][c]);
+                    });
                 });
                 __syncthreads();
             }
@@ -353,39 +420,34 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
         // Epilogue: bra Cartesian -> spherical, coalesced packed stores.
         const size_t obase = (size_t)__ldg(map.out_begin + m);
         double wsum = 0.0;
-        static_for<0, C::KS>([&](auto g) {
-            constexpr int G = decltype(g)::value;
-            if (warp == G) {
-                static_for<0, C::KPW>([&](auto c_) {
-                    constexpr int c = decltype(c_)::value;
-                    constexpr int ko = G * C::KPW + c;
-                    if constexpr (ko < C::NKO) {
-                        static_for<0, nsph(LI)>([&](auto I_) {
-                            constexpr int I = decltype(I_)::value;
-                            static_for<0, nsph(LJ)>([&](auto J_) {
-                                constexpr int J = decltype(J_)::value;
-                                double v = 0.0;
-                                static_for<0, C::NI>([&](auto ci_) {
-                                    constexpr int ci = decltype(ci_)::value;
-                                    constexpr double wi = sph_coef(LI, I, ci);
-                                    if constexpr (wi != 0.0) {
-                                        double vj = 0.0;
-                                        static_for<0, C::NJ>([&](auto cj_) {
-                                            constexpr int cj = decltype(cj_)::value;
-                                            constexpr double wj = sph_coef(LJ, J, cj);
-                                            if constexpr (wj != 0.0) vj = fma(wj, acc[ci * C::NJ + cj][c], vj);
-                                        });
-                                        v = fma(wi, vj, v);
-                                    }
+        static_for<0, C::KPW>([&](auto c_) {
+            constexpr int c = decltype(c_)::value;
+            const int ko = warp * C::KPW + c;
+            if (ko < C::NKO) {
+                static_for<0, nsph(LI)>([&](auto I_) {
+                    constexpr int I = decltype(I_)::value;
+                    static_for<0, nsph(LJ)>([&](auto J_) {
+                        constexpr int J = decltype(J_)::value;
+                        double v = 0.0;
+                        static_for<0, C::NI>([&](auto ci_) {
+                            constexpr int ci = decltype(ci_)::value;
+                            constexpr double wi = sph_coef(LI, I, ci);
+                            if constexpr (wi != 0.0) {
+                                double vj = 0.0;
+                                static_for<0, C::NJ>([&](auto cj_) {
+                                    constexpr int cj = decltype(cj_)::value;
+                                    constexpr double wj = sph_coef(LJ, J, cj);
+                                    if constexpr (wj != 0.0) vj = fma(wj, acc[ci * C::NJ + cj][c], vj);
                                 });
-                                if (valid) {
-                                    const size_t row = ((size_t)sp_local * C::NIJS + I * nsph(LJ) + J) * C::NKO + ko;
-                                    out[obase + row * n_aux + a_local] = v;
-                                    wsum += v;
-                                }
-                            });
+                                v = fma(wi, vj, v);
+                            }
                         });
-                    }
+                        if (valid) {
+                            const size_t row = ((size_t)sp_local * C::NIJS + I * nsph(LJ) + J) * C::NKO + ko;
+                            out[obase + row * n_aux + a_local] = v;
+                            wsum += v;
+                        }
+                    });
                 });
             }
         });
@@ -398,22 +460,23 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
 }
 
 // Occupancy-sized persistent grid for one class.
-template <int LI, int LJ, int LK>
+template <int LI, int LJ, int LK, int V>
 static int launch_one(const double* boys_table, const BraTable& bra, const KetTable& ket, const BatchMap& map,
                       int total_items, double omega, double* out, int* counter, cudaStream_t s) {
-    using C = Fast3c<LI, LJ, LK>;
+    using C = Fast3c<LI, LJ, LK, V>;
     if (total_items <= 0) return 0;
     static int max_blocks = 0;
     if (max_blocks == 0) {
         int per_sm = 0, dev = 0, sms = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3c_fast<LI, LJ, LK>, C::THREADS, 0) != cudaSuccess)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3c_fast<LI, LJ, LK, V>, C::THREADS, 0) !=
+            cudaSuccess)
             return 2;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         max_blocks = (per_sm < 1 ? 1 : per_sm) * sms;
     }
     const int blocks = total_items < max_blocks ? total_items : max_blocks;
-    k3c_fast<LI, LJ, LK><<<blocks, C::THREADS, 0, s>>>(boys_table, bra, ket, map, omega, out, counter, total_items);
+    k3c_fast<LI, LJ, LK, V><<<blocks, C::THREADS, 0, s>>>(boys_table, bra, ket, map, omega, out, counter, total_items);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 

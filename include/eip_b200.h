@@ -79,6 +79,14 @@ unsigned long long eip_kernel_launch_count(void);
  * last reference-ABI call, in milliseconds. */
 float eip_last_kernel_ms(void);
 
+/* Tuning variant (0..3) of the fast (mu nu|P) kernel of class (i_L, j_L | k_L),
+ * i_L <= j_L <= 2, k_L <= 4: accumulator budget and register cap (see
+ * k3c_fast.cuh).  Affects launches made after the call (a batch's graph keeps
+ * the variants it was captured with).  set returns 1 for an invalid
+ * class/variant; get returns -1 for a class without fast kernels. */
+int eip_tune_set(int i_L, int j_L, int k_L, int variant);
+int eip_tune_get(int i_L, int j_L, int k_L);
+
 /* Device Boys function: F[i*(L+1)+m] = F_m(T[i]), m = 0..L <= 21 (host buffers). */
 int eip_boys(int L, const double* T, int n, double* F);
 

@@ -71,3 +71,26 @@ def test_batch_checksums_and_rerun(small_batch):
     b._check(b.L.eip_batch_copy_output(b.h, 0, b.output_elems, out2.ctypes.data_as(
         __import__("ctypes").POINTER(__import__("ctypes").c_double))), "copy")
     assert np.array_equal(out, out2)
+
+
+def test_every_tuning_variant_matches_reference(small_batch):
+    """All compiled variants of every fast class give the same integrals."""
+    mols, pds, ads, b = small_batch
+    ref = oracle.reference()
+    if ref is None:
+        pytest.skip("reference library not built")
+    lm = importlib.import_module("electron-integral-playground_b200._lib")
+    L = lm.lib()
+    want = oracle.drive_three_center(ref, pds[3], ads[3], mols[3])
+    saved = {(li, lj, lk): L.eip_tune_get(li, lj, lk) for (li, lj) in pds[3] for lk in ads[3]}
+    try:
+        for v in range(4):
+            for (li, lj, lk) in saved:
+                if saved[(li, lj, lk)] >= 0:
+                    L.eip_tune_set(li, lj, lk, v)
+            got = mi.three_center(pds[3], ads[3], mols[3])
+            np.testing.assert_allclose(got, want, rtol=0, atol=1e-12, err_msg=f"variant {v}")
+    finally:
+        for k, v in saved.items():
+            if v >= 0:
+                L.eip_tune_set(*k, v)
