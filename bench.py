@@ -129,6 +129,42 @@ class ClockSampler:
                 "power_w_max": max(float(r[3]) for r in rows)}
 
 
+def mixed_error(bt, mols, pds, ads, threshold, torch, budget_bytes=30e9):
+    """Max |mixed - FP64| over the packed (mu nu|P) of the leading molecules whose
+    output fits budget_bytes (both results resident at once)."""
+    take, total = [], 0
+    for i, m in enumerate(mols):
+        b = 8 * m.n_ao * m.n_ao * m.n_aux  # dense size; the packed output is about half
+        if total + b > 2 * budget_bytes:
+            break
+        take.append(i)
+        total += b
+    sub = [mols[i] for i in take], [pds[i] for i in take], [ads[i] for i in take]
+    f64 = bt.ThreeCenterBatch(*sub, precision="fp64")
+    mix = bt.ThreeCenterBatch(*sub, precision="mixed", fp32_threshold=threshold)
+    n = f64.output_elems
+    a = torch.empty(n, dtype=torch.float64, device="cuda")
+    c = torch.empty(n, dtype=torch.float64, device="cuda")
+    f64.bind_output(a.data_ptr())
+    mix.bind_output(c.data_ptr())
+    f64.run()
+    mix.run()
+    f64.status()
+    mix.status()
+    d = (a - c).abs()
+    big = a.abs() > 1e-6
+    rel = float(((a - c).abs() / a.abs().clamp_min(1e-300))[big].max()) if bool(big.any()) else 0.0
+    out = {"max_abs": float(d.max()), "max_rel_where_abs_gt_1e-6": rel, "molecules": len(take),
+           "elements": n}
+    f64.bind_output(0)
+    mix.bind_output(0)
+    f64.close()
+    mix.close()
+    del a, c
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference_arm(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -166,6 +202,8 @@ def main():
     ap.add_argument("--molecules", type=int, default=64)
     ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of reference CPU work per sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp32-threshold", type=float, default=1e-3,
+                    help="mixed precision: FP32 for shell pairs with bound below this")
     ap.add_argument("--tune", action="store_true",
                     help="run the autotuner on this workload first and rewrite its cache")
     args = ap.parse_args()
@@ -196,85 +234,110 @@ def main():
 
     mols, pds, ads, stats = build_workload(args.seed + 1000 * rank, args.molecules)
     tot, per_class = rf.totals(stats)
-    batch = bt.ThreeCenterBatch(mols, pds, ads)
-    free, total_mem = torch.cuda.mem_get_info()
+    batch = bt.ThreeCenterBatch(mols, pds, ads, precision="fp64")
+    free, _ = torch.cuda.mem_get_info()
     if batch.output_bytes > free - (2 << 30):
         raise RuntimeError(f"packed output {batch.output_bytes / 1e9:.1f} GB exceeds free device memory")
     batch.alloc_output()
-    stream = torch.cuda.ExternalStream(batch.stream)
+    out_ptr = batch.L.eip_batch_output_device(batch.h)
     tuning = at.load()
     if args.tune:
         table, timings = at.tune(batch, sorted(per_class))
         at.save(table, timings, {"workload": WORKLOAD, "seed": args.seed, "molecules": args.molecules,
                                  "gpu": torch.cuda.get_device_name(local)})
         tuning = at.load()
+    mixed = bt.ThreeCenterBatch(mols, pds, ads, precision="mixed", fp32_threshold=args.fp32_threshold)
+    mixed.bind_output(out_ptr)  # same layout; the two paths run one after the other
+    table_bytes = {"fp64": batch.table_bytes, "mixed": mixed.table_bytes}
+    out_bytes = batch.output_bytes
 
-    def timed(fn, k):
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        per = []
+    def measure(b, clocks_path):
+        """K graph launches timed with CUDA events on b's stream (value), then K
+        end-to-end steps (H2D tables + graph + D2H checksums)."""
+        stream = torch.cuda.ExternalStream(b.stream)
+        for _ in range(args.warmup):
+            b.run(sync=False)
         torch.cuda.synchronize()
-        if world > 1:
-            torch.distributed.barrier()
-        ev0.record(stream)
-        marks = []
-        for _ in range(k):
-            e = torch.cuda.Event(enable_timing=True)
-            fn()
-            e.record(stream)
-            marks.append(e)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        last = ev0
-        for e in marks:
-            per.append(last.elapsed_time(e))
-            last = e
-        total = ev0.elapsed_time(ev1)
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        with ClockSampler(clocks_path) as cs:
+            if world > 1:
+                torch.distributed.barrier()
+            marks[0].record(stream)
+            for k in range(args.steps):
+                b.run(sync=False)
+                marks[k + 1].record(stream)
+            torch.cuda.synchronize()
+        per_step = [marks[k].elapsed_time(marks[k + 1]) for k in range(args.steps)]
+        total = marks[0].elapsed_time(marks[-1])
         if world > 1:
             t = torch.tensor([total], device="cuda")
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             total = float(t.item())
-        return total, per
+        b.status()
+        h_ck = np.empty(len(mols))
 
-    for _ in range(args.warmup):
-        batch.run(sync=False)
-    torch.cuda.synchronize()
-    clocks_path = str(REPO / "gpurun_out" / f"clocks_rank{rank}.csv") if (REPO / "gpurun_out").is_dir() else \
-        f"/tmp/eip_clocks_{os.getpid()}.csv"
-    with ClockSampler(clocks_path) as cs:
-        total_ms, per_step = timed(lambda: batch.run(sync=False), args.steps)
-    clocks = cs.summary(local)
+        def e2e_step():
+            b.upload()
+            b.run(checksum=True, sync=False)
+            b._check(b.L.eip_batch_checksums(b.h, lm.dp(h_ck)), "checksums")
 
-    # e2e: H2D of every input table + graph + D2H of the per-molecule checksums.
-    h_ck = np.empty(len(mols))
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) * 1e3 / args.steps
+        e2e = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([e2e], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e = float(t.item())
+        return {"ms": total / args.steps, "per_step": per_step, "e2e_ms": e2e, "e2e_wall_ms": wall,
+                "clocks": cs.summary(local), "launches": b.launches_per_run * args.steps}
 
-    def e2e_step():
-        batch.upload()
-        batch.run(checksum=True, sync=False)
-        batch._check(batch.L.eip_batch_checksums(batch.h, lm.dp(h_ck)), "checksums")
+    gdir = REPO / "gpurun_out"
+    cpath = (lambda tag: str(gdir / f"clocks_{tag}_rank{rank}.csv")) if gdir.is_dir() else \
+        (lambda tag: f"/tmp/eip_clocks_{tag}_{os.getpid()}.csv")
+    m64 = measure(batch, cpath("fp64"))
+    mmix = measure(mixed, cpath("mixed"))
+    split64 = split32 = 0
+    for (li, lj, lk) in per_class:
+        sp = mixed.precision_split(li, lj, lk)
+        if sp:
+            split64 += sp[0]
+            split32 += sp[1]
+    mixed.bind_output(0)
+    mixed.close()
 
-    for _ in range(2):
-        e2e_step()
-    t0 = time.perf_counter()
-    e2e_ms, _ = timed(e2e_step, args.steps)
-    e2e_wall_ms = (time.perf_counter() - t0) * 1e3
-
-    # Per-class device time (each class kernel alone, 2 launches, CUDA events).
+    # Per-class device time (each FP64 class kernel alone, 2 launches, CUDA events).
+    stream = torch.cuda.ExternalStream(batch.stream)
     class_ms = {}
     for (li, lj, lk) in sorted(per_class):
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if not batch.run_class(li, lj, lk):
             continue
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         for _ in range(2):
             batch.run_class(li, lj, lk)
         ev1.record(stream)
         torch.cuda.synchronize()
         class_ms[(li, lj, lk)] = ev0.elapsed_time(ev1) / 2
+    batch.status()
     fp64_peak = bt.measure_fma_peak(True)
+    fp32_peak = bt.measure_fma_peak(False)
+    batch.close()
+    torch.cuda.empty_cache()
+    err = mixed_error(bt, mols, pds, ads, args.fp32_threshold, torch)
+    mixed_ok = err["max_abs"] <= 1e-10
+    head = mmix if mixed_ok else m64
 
     screened = tot["screened"] * world
-    ms_step = total_ms / args.steps
-    value = screened / (ms_step * 1e-3)
+    value = screened / (head["ms"] * 1e-3)
     dom = max(class_ms, key=class_ms.get) if class_ms else None
     roof = None
     if dom:
@@ -285,46 +348,55 @@ def main():
             for line in tfile.read_text().splitlines():
                 if line.startswith(f"dram_bytes_per_launch {dom[0]}{dom[1]}{dom[2]} "):
                     traffic = float(line.split()[2])
-        roof = {"bound": "fp64", "kernel": f"k3c_fast<{dom[0]},{dom[1]},{dom[2]}>", "achieved": achieved,
+        roof = {"bound": "fp64", "kernel": f"k3c_fast<{dom[0]},{dom[1]},{dom[2]}> (FP64)", "achieved": achieved,
                 "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic,
                 "peak_source": "FP64 FMA microbenchmark on this GPU (eip_measure_fma_peak), this run",
                 "algorithmic_flops_per_launch": per_class[dom]["flops"], "ms_per_launch": class_ms[dom],
-                "whole_step_tflops": tot["flops"] / (ms_step * 1e-3) / 1e12,
-                "whole_step_frac": tot["flops"] / (ms_step * 1e-3) / 1e12 / fp64_peak,
-                "output_store_gbs": tot["out_bytes"] / (ms_step * 1e-3) / 1e9}
+                "whole_step_tflops_fp64": tot["flops"] / (m64["ms"] * 1e-3) / 1e12,
+                "whole_step_frac_fp64": tot["flops"] / (m64["ms"] * 1e-3) / 1e12 / fp64_peak,
+                "output_store_gbs": tot["out_bytes"] / (head["ms"] * 1e-3) / 1e9}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        s = reference_sample(mols, pds, ads, stats, args.ref_budget)
-        if s is not None:
-            cpu = {"value": s["value"], "unit": UNIT, "cores": s["cores"], "kind": "reference",
-                   "sample": f"molecules {s['molecules']} of the batch (dense output <= 2e8 doubles each), "
-                             f"{s['triplets']} screened triplets, {s['seconds']:.1f} s"}
+        smp = reference_sample(mols, pds, ads, stats, args.ref_budget)
+        if smp is not None:
+            cpu = {"value": smp["value"], "unit": UNIT, "cores": smp["cores"], "kind": "reference",
+                   "sample": f"molecules {smp['molecules']} of the batch (dense output <= 2e8 doubles each), "
+                             f"{smp['triplets']} screened triplets, {smp['seconds']:.1f} s"}
     if rank == 0:
+        per = head["per_step"]
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators; no dataset)",
+            "warmup": args.warmup, "ms_per_step": head["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32 (mixed)" if mixed_ok else "f64",
+            "data": "synthetic (seeded generators; no dataset)",
             "config": {"workload": WORKLOAD, "molecules": args.molecules * world, "seed": args.seed,
-                       "atoms": sum(len(m.elements) for m in mols) * world, "precision": "fp64",
+                       "atoms": sum(len(m.elements) for m in mols) * world,
+                       "precision": "mixed" if mixed_ok else "fp64",
                        "classes": len(per_class), "primitive_triplets_per_step": tot["primitive"] * world,
                        "contracted_triplets_per_step": tot["contracted"] * world,
                        "screened_triplets_per_step": screened, "threshold": THRESHOLD,
-                       "packed_output_bytes": batch.output_bytes, "input_table_bytes": batch.table_bytes,
+                       "packed_output_bytes": out_bytes, "input_table_bytes": table_bytes,
                        "l2": "inputs + packed output per step exceed the 126 MB L2 (no flush needed)",
                        "parallelism": f"{world} independent shard(s)"},
-            "e2e": {"value": screened / (e2e_ms / args.steps * 1e-3), "unit": UNIT,
-                    "h2d_bytes_per_step": batch.table_bytes, "d2h_bytes_per_step": 8 * len(mols),
-                    "wall_ms_per_step": e2e_wall_ms / args.steps,
+            "precision": {"fp64_value": screened / (m64["ms"] * 1e-3), "fp64_ms_per_step": m64["ms"],
+                          "mixed_value": screened / (mmix["ms"] * 1e-3), "mixed_ms_per_step": mmix["ms"],
+                          "fp32_threshold": args.fp32_threshold,
+                          "fp32_fraction_of_triplets": split32 / max(1, split32 + split64),
+                          "mixed_vs_fp64_error": err, "fp32_fma_peak_tflops": fp32_peak,
+                          "headline": "mixed" if mixed_ok else "fp64"},
+            "e2e": {"value": screened / (head["e2e_ms"] * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": table_bytes["mixed" if mixed_ok else "fp64"],
+                    "d2h_bytes_per_step": 8 * len(mols),
+                    "wall_ms_per_step": head["e2e_wall_ms"],
+                    "fp64_value": screened / (m64["e2e_ms"] * 1e-3),
                     "result": "per-molecule checksum of the packed (mu nu|P) (computed in the kernels' epilogue)"},
             "roofline": roof, "cpu_baseline": cpu,
-            "gpu_launches": batch.launches_per_run * args.steps, "clocks": clocks,
-            "latency_ms": {"p50": statistics.median(per_step),
-                           "p99": sorted(per_step)[min(len(per_step) - 1, int(0.99 * len(per_step)))]},
+            "gpu_launches": head["launches"], "clocks": head["clocks"], "clocks_fp64": m64["clocks"],
+            "latency_ms": {"p50": statistics.median(per), "p99": sorted(per)[min(len(per) - 1, int(0.99 * len(per)))]},
             "class_ms": {f"{k[0]}{k[1]}|{k[2]}": round(v, 4) for k, v in sorted(class_ms.items())},
             "tuning": "autotuned variants (tuning/b200_fp64.json)" if tuning else "default variants",
         }
         print(json.dumps(line))
-    batch.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

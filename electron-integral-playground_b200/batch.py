@@ -28,6 +28,8 @@ def _bind(L):
     L.eip_batch_add_pairs.argtypes = [_vp, c_int, c_int, c_int, _dpp, _dpp, _dpp, _dpp, _ipp, _ipp, c_int]
     L.eip_batch_add_aux.argtypes = [_vp, c_int, c_int, _dpp, _dpp, _ipp, c_int]
     L.eip_batch_build.argtypes = [_vp]
+    L.eip_batch_set_precision.argtypes = [_vp, c_int, c_double]
+    L.eip_batch_precision_split.argtypes = [_vp, c_int, c_int, c_int, ctypes.POINTER(c_ll), ctypes.POINTER(c_ll)]
     L.eip_batch_output_elems.argtypes = [_vp]
     L.eip_batch_output_elems.restype = c_ll
     L.eip_batch_block.argtypes = [_vp, c_int, c_int, c_int, c_int, ctypes.POINTER(c_ll), _ipp, _ipp]
@@ -55,8 +57,16 @@ def _bind(L):
     L._batch_bound = True
 
 
+DEFAULT_FP32_THRESHOLD = 1e-3
+
+
 class ThreeCenterBatch:
-    def __init__(self, molecules, pair_data_list, aux_data_list, omega: float = 0.0):
+    """precision: "fp64", or "mixed" (FP32 R/ket/bra for shell pairs whose
+    bound Q_pair * max Q_aux (times the output-transform gains) is below
+    fp32_threshold; FP64 Boys, E recurrences, prefactors and every other pair)."""
+
+    def __init__(self, molecules, pair_data_list, aux_data_list, omega: float = 0.0, precision: str = "fp64",
+                 fp32_threshold: float = DEFAULT_FP32_THRESHOLD):
         if not (len(molecules) == len(pair_data_list) == len(aux_data_list)) or not molecules:
             raise ValueError("need one pair table and one auxiliary table per molecule")
         spherical = {bool(m.spherical_basis) for m in molecules}
@@ -72,6 +82,11 @@ class ThreeCenterBatch:
         self.h = self.L.eip_batch_create(len(molecules), self.spherical, self.omega)
         if not self.h:
             raise IntegralError("eip_batch_create failed")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.precision = precision
+        self._check(self.L.eip_batch_set_precision(self.h, 1 if precision == "mixed" else 0, float(fp32_threshold)),
+                    "set_precision")
         self._keep = []
         for m, (pd, ad) in enumerate(zip(pair_data_list, aux_data_list)):
             for (li, lj), p in pd.items():
@@ -147,6 +162,13 @@ class ThreeCenterBatch:
         out = np.empty(len(self.molecules))
         self._check(self.L.eip_batch_checksums(self.h, dp(out)), "checksums")
         return out
+
+    def precision_split(self, li, lj, lk):
+        """(FP64 triplets, FP32 triplets) of one class."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        if self.L.eip_batch_precision_split(self.h, li, lj, lk, ctypes.byref(a), ctypes.byref(b)) != 0:
+            return None
+        return a.value, b.value
 
     def block(self, m, li, lj, lk):
         off, nsp, nax = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int()

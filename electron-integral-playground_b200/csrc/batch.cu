@@ -45,6 +45,12 @@ struct ClassPlan {
     KetTable ket{};
     BatchMap map{};
     int* counter = nullptr;
+    // mixed precision: FP32 work list (shell pairs under the bound threshold)
+    int total_items32 = 0;
+    BatchMap map32{};
+    int* counter32 = nullptr;
+    long long triplets32 = 0, triplets64 = 0;
+    int n_sp_total32 = 0;
     std::vector<long long> out_begin;   // per molecule
     std::vector<int> n_sp, n_auxsh;     // per molecule
     std::vector<int> sp0, aux0;         // per molecule (global indices in class tables)
@@ -75,6 +81,8 @@ struct eip_batch {
     int n_mol = 0;
     bool spherical = true;
     double omega = 0.0;
+    int precision = 0;     // 0 FP64, 1 mixed (FP32 for bounded shell pairs)
+    double fp32_tau = 0.0;
     std::vector<std::map<std::pair<int, int>, PairIn>> pairs;  // per molecule
     std::vector<std::map<int, AuxIn>> aux;                     // per molecule
     bool built = false;
@@ -133,9 +141,53 @@ void group_indices(const int* ia, const int* ja, int n, std::vector<int>& order,
     begin.push_back(n);
 }
 
+// Upper bound of |(ab|ab)|^(1/2) and of the overlap of one primitive pair, the
+// construction of the reference front end (pair_utility.py:38-66) with the
+// distance shift applied once: 2 |c_a c_b| (la/2ea)^(la/2) (lb/2eb)^(lb/2)
+// exp(-ab/p d^2) max((pi/p)^1.5, 2^0.25 (pi/p)^1.25), d = max(|AB| - sqrt(la/2a)
+// - sqrt(lb/2b), 0); |c_a c_b| recovered from c_ab = c_a c_b exp(-ab/p |AB|^2).
+double pair_bound(const double* A, const double* B, double coef, int la, int lb) {
+    const double a = A[3], b = B[3], p = a + b, mu = a * b / p;
+    const double dx = A[0] - B[0], dy = A[1] - B[1], dz = A[2] - B[2];
+    const double ab2 = dx * dx + dy * dy + dz * dz, ab = sqrt(ab2);
+    double d = ab - sqrt(la / (2.0 * a)) - sqrt(lb / (2.0 * b));
+    if (d < 0.0) d = 0.0;
+    double f = 2.0 * fabs(coef) * exp(mu * (ab2 - d * d));
+    if (la > 0) f *= pow(la / (2.0 * M_E * a), la / 2.0);
+    if (lb > 0) f *= pow(lb / (2.0 * M_E * b), lb / 2.0);
+    return f * fmax(pow(M_PI / p, 1.5), pow(2.0, 0.25) * pow(M_PI / p, 1.25));
+}
+
+// Same construction for one auxiliary primitive: |c| 2 (l/2eq)^(l/2) (2 pi^(5/2) / (q^2 sqrt(2q)))^(1/2).
+double aux_bound(double q, double coef, int l) {
+    double f = 2.0 * fabs(coef) * sqrt(2.0 * pow(M_PI, 2.5) / (q * q * sqrt(2.0 * q)));
+    if (l > 0) f *= pow(l / (2.0 * M_E * q), l / 2.0);
+    return f;
+}
+
+// Largest sum of |coefficients| of a row of the output transform of one l.
+double transform_gain(int l, bool spherical) {
+    double g = 1.0;
+    for (int m = 0; m < (spherical ? nsph(l) : ncart(l)); m++) {
+        double r = 0.0;
+        for (int c = 0; c < ncart(l); c++)
+            r += spherical ? fabs(eip_sph_coef[eip_sph_offset[l] + m * ncart(l) + c])
+                           : (m == c ? eip_cart_norm[eip_cart_norm_offset[l] + c] : 0.0);
+        g = fmax(g, r);
+    }
+    return g;
+}
+
 }  // namespace
 
 extern "C" {
+
+int eip_batch_set_precision(eip_batch* b, int mode, double fp32_threshold) {
+    if (!b || b->built || mode < 0 || mode > 1 || !(fp32_threshold >= 0.0)) return 2;
+    b->precision = mode;
+    b->fp32_tau = fp32_threshold;
+    return 0;
+}
 
 eip_batch* eip_batch_create(int n_molecules, bool spherical, double omega) {
     if (n_molecules <= 0 || omega < 0.0) return nullptr;
@@ -193,12 +245,14 @@ int eip_batch_build(eip_batch* b) {
         std::vector<int2> ao;
         std::vector<double4> AB, P, PA;
         std::vector<int> sp_begin;  // per molecule prefix (n_mol + 1)
+        std::vector<double> bound;  // per shell pair: sum of primitive pair bounds
     };
     struct KetHost {
         std::vector<int> begin, start;
         std::vector<double4> C;
         std::vector<double> coef;
         std::vector<int> aux_begin;
+        std::vector<double> max_bound;  // per molecule: largest auxiliary shell bound
     };
     std::map<std::pair<int, int>, BraHost> bh;
     std::map<int, KetHost> kh;
@@ -220,6 +274,12 @@ int eip_batch_build(eip_batch* b) {
                     H.AB.push_back(make_double4(p.A[4 * q] - p.B[4 * q], p.A[4 * q + 1] - p.B[4 * q + 1],
                                                 p.A[4 * q + 2] - p.B[4 * q + 2], 0.0));
                     H.begin.push_back(prim0 + gb[g + 1]);
+                    double qb = 0.0;
+                    for (int k = gb[g]; k < gb[g + 1]; k++) {
+                        const int r = order[k];
+                        qb += pair_bound(&p.A[4 * r], &p.B[4 * r], p.coef[r], pc.first.first, pc.first.second);
+                    }
+                    H.bound.push_back(qb);
                 }
                 for (int k = 0; k < n; k++) {
                     const int q = order[k];
@@ -237,6 +297,7 @@ int eip_batch_build(eip_batch* b) {
         H.begin.push_back(0);
         H.aux_begin.push_back(0);
         for (int m = 0; m < b->n_mol; m++) {
+            double qmax = 0.0;
             auto it = b->aux[m].find(ac.first);
             if (it != b->aux[m].end() && !it->second.start.empty()) {
                 const AuxIn& a = it->second;
@@ -246,6 +307,9 @@ int eip_batch_build(eip_batch* b) {
                 for (size_t g = 0; g + 1 < gb.size(); g++) {
                     H.start.push_back(gi[g]);
                     H.begin.push_back(prim0 + gb[g + 1]);
+                    double qa = 0.0;
+                    for (int k = gb[g]; k < gb[g + 1]; k++) qa += aux_bound(a.C[4 * order[k] + 3], a.coef[order[k]], ac.first);
+                    qmax = fmax(qmax, qa);
                 }
                 for (int k = 0; k < n; k++) {
                     const int q = order[k];
@@ -253,6 +317,7 @@ int eip_batch_build(eip_batch* b) {
                     H.coef.push_back(a.coef[q]);
                 }
             }
+            H.max_bound.push_back(qmax);
             H.aux_begin.push_back((int)H.start.size());
         }
     }
@@ -307,9 +372,57 @@ int eip_batch_build(eip_batch* b) {
                               L.add(sizeof(double4) * H.C.size()), L.add(sizeof(double) * H.coef.size()),
                               L.add(sizeof(int) * H.aux_begin.size())};
     }
-    std::vector<size_t> plan_off;
-    for (auto& pl : b->plans) {
-        plan_off.push_back(L.add(sizeof(int) * (3 * (b->n_mol + 1) + 2) + sizeof(long long) * (b->n_mol + 1)));
+    // Per-plan work maps: ints = [item_begin64 | list_begin64 | aux_begin | item_begin32 |
+    // list_begin32 | sp_first] (n_mol + 1 each), 4 counters/status words, the
+    // FP64 and FP32 shell-pair lists; then the 8-byte aligned out_begin array.
+    const int nm = b->n_mol;
+    std::vector<std::vector<int>> plan_ints(b->plans.size());
+    std::vector<size_t> plan_off, plan_ob;
+    for (size_t i = 0; i < b->plans.size(); i++) {
+        ClassPlan& pl = b->plans[i];
+        const BraHost& B = bh[{pl.li, pl.lj}];
+        const KetHost& K = kh[pl.lk];
+        const bool mixed = b->precision == 1 && pl.fast;
+        const double gain = transform_gain(pl.li, b->spherical) * transform_gain(pl.lj, b->spherical) *
+                            transform_gain(pl.lk, b->spherical);
+        std::vector<int>& v = plan_ints[i];
+        v.assign(6 * (nm + 1) + 4, 0);
+        int* ib64 = &v[0];
+        int* lb64 = &v[nm + 1];
+        int* axb = &v[2 * (nm + 1)];
+        int* ib32 = &v[3 * (nm + 1)];
+        int* lb32 = &v[4 * (nm + 1)];
+        int* spf = &v[5 * (nm + 1)];
+        std::vector<int> list64, list32;
+        for (int m = 0; m < nm; m++) {
+            const int tiles = (pl.n_auxsh[m] + 31) / 32;
+            int n64 = 0, n32 = 0;
+            for (int g = B.sp_begin[m]; g < B.sp_begin[m + 1]; g++) {
+                const bool f32 = mixed && B.bound[g] * K.max_bound[m] * gain < b->fp32_tau;
+                (f32 ? list32 : list64).push_back(g);
+                (f32 ? n32 : n64)++;
+            }
+            pl.triplets32 += (long long)n32 * pl.n_auxsh[m];
+            pl.triplets64 += (long long)n64 * pl.n_auxsh[m];
+            ib64[m + 1] = ib64[m] + n64 * tiles;
+            ib32[m + 1] = ib32[m] + n32 * tiles;
+            lb64[m + 1] = lb64[m] + n64;
+            lb32[m + 1] = lb32[m] + n32;
+        }
+        for (int m = 0; m <= nm; m++) {
+            axb[m] = K.aux_begin[m];
+            spf[m] = B.sp_begin[m];
+        }
+        if ((long long)ib64[nm] > 0x7fffffffLL || (long long)ib32[nm] > 0x7fffffffLL)
+            return fail(b, "too many work items in one class", cudaSuccess);
+        pl.total_items = ib64[nm];
+        pl.total_items32 = ib32[nm];
+        pl.n_sp_total32 = (int)list32.size();
+        v.insert(v.end(), list64.begin(), list64.end());
+        v.insert(v.end(), list32.begin(), list32.end());
+        const size_t ints_bytes = (sizeof(int) * v.size() + 7) & ~size_t(7);
+        plan_off.push_back(L.add(ints_bytes + sizeof(long long) * nm));
+        plan_ob.push_back(plan_off.back() + ints_bytes);
     }
     size_t etab_total = 0;
     for (auto& kv : bh) {
@@ -358,29 +471,27 @@ int eip_batch_build(eip_batch* b) {
     }
     for (size_t i = 0; i < b->plans.size(); i++) {
         ClassPlan& pl = b->plans[i];
-        const int nm = b->n_mol;
-        int* hp = at<int>(h, plan_off[i]);
+        const std::vector<int>& v = plan_ints[i];
+        memcpy(at<int>(h, plan_off[i]), v.data(), sizeof(int) * v.size());
+        memcpy(at<long long>(h, plan_ob[i]), pl.out_begin.data(), sizeof(long long) * nm);
         int* dp = at<int>(d, plan_off[i]);
-        int* item_begin = hp;
-        int* sp_begin = hp + (nm + 1);
-        int* aux_begin = hp + 2 * (nm + 1);
-        hp[3 * (nm + 1)] = 0;      // work counter
-        hp[3 * (nm + 1) + 1] = 0;  // kernel self-check status
-        item_begin[0] = 0;
-        for (int m = 0; m < nm; m++)
-            item_begin[m + 1] = item_begin[m] + pl.n_sp[m] * ((pl.n_auxsh[m] + 31) / 32);
-        for (int m = 0; m <= nm; m++) {
-            sp_begin[m] = b->bra_sp_begin[{pl.li, pl.lj}][m];
-            aux_begin[m] = b->ket_aux_begin[pl.lk][m];
-        }
-        // 8-byte aligned out_begin right after the ints
-        const size_t ints = 3 * (nm + 1) + 2;
-        const size_t ob_off = plan_off[i] + ((sizeof(int) * ints + 7) & ~size_t(7));
-        memcpy(at<long long>(h, ob_off), pl.out_begin.data(), sizeof(long long) * nm);
+        const long long* dob = at<long long>(d, plan_ob[i]);
+        const bool mixed = b->precision == 1 && pl.fast;
+        int* counters = dp + 6 * (nm + 1);
+        const int* list64 = counters + 4;
+        const int* list32 = list64 + (v.size() - 6 * (nm + 1) - 4) - pl.n_sp_total32;
         pl.bra = b->bra_by_class[{pl.li, pl.lj}];
         pl.ket = ket_by_class[pl.lk];
-        pl.counter = dp + 3 * (nm + 1);
-        pl.map = BatchMap{nm, dp, dp + (nm + 1), dp + 2 * (nm + 1), at<long long>(d, ob_off), nullptr};
+        pl.counter = counters;
+        pl.counter32 = counters + 2;
+        if (mixed) {
+            pl.map = BatchMap{nm, dp, dp + (nm + 1), dp + 2 * (nm + 1), dob, nullptr, list64, dp + 5 * (nm + 1)};
+            pl.map32 = BatchMap{nm, dp + 3 * (nm + 1), dp + 4 * (nm + 1), dp + 2 * (nm + 1), dob, nullptr, list32,
+                                dp + 5 * (nm + 1)};
+        } else {
+            // all pairs in FP64: plain numbering, sp_begin = the molecule's first pair
+            pl.map = BatchMap{nm, dp, dp + 5 * (nm + 1), dp + 2 * (nm + 1), dob, nullptr, nullptr, nullptr};
+        }
     }
     if ((e = cudaMemcpyAsync(d, h, L.total, cudaMemcpyHostToDevice, b->stream)) != cudaSuccess)
         return fail(b, "table upload", e);
@@ -454,7 +565,7 @@ static int capture(eip_batch* b, bool checksum) {
     int rc = 0;
     cudaMemsetAsync(b->d_checksum, 0, sizeof(double) * b->n_mol, b->stream);
     for (ClassPlan& pl : b->plans)
-        if (pl.fast) cudaMemsetAsync(pl.counter, 0, 2 * sizeof(int), b->stream);
+        if (pl.fast) cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), b->stream);
     for (auto& kv : b->bra_by_class) {
         if (!fast3c_supported(kv.first.first, kv.first.second, 0) || !b->spherical) continue;
         rc |= launch_e_table(kv.first.first, kv.first.second, kv.second, b->d_etab + b->etab_offset[kv.first],
@@ -465,14 +576,23 @@ static int capture(eip_batch* b, bool checksum) {
     for (int i = 0; i < n_side; i++) cudaStreamWaitEvent(b->side[i], b->events[0], 0);
     int next = 0;
     for (ClassPlan& pl : b->plans) {
-        if (pl.total_items == 0) continue;
+        if (pl.total_items == 0 && pl.total_items32 == 0) continue;
         cudaStream_t s = b->side[next++ % n_side];
         if (pl.fast) {
-            BatchMap map = pl.map;
-            map.checksum = checksum ? b->d_checksum : nullptr;
-            rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, map, pl.total_items, b->omega, b->d_out,
-                                pl.counter, s);
-            launches++;
+            if (pl.total_items > 0) {
+                BatchMap map = pl.map;
+                map.checksum = checksum ? b->d_checksum : nullptr;
+                rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, map, pl.total_items, b->omega, b->d_out,
+                                    pl.counter, s);
+                launches++;
+            }
+            if (pl.total_items32 > 0) {
+                BatchMap map = pl.map32;
+                map.checksum = checksum ? b->d_checksum : nullptr;
+                rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, map, pl.total_items32, b->omega, b->d_out,
+                                    pl.counter32, s, true);
+                launches++;
+            }
         } else {
             for (int m = 0; m < b->n_mol; m++) {
                 if (pl.n_sp[m] == 0 || pl.n_auxsh[m] == 0) continue;
@@ -517,12 +637,31 @@ int eip_batch_run_class(eip_batch* b, int i_L, int j_L, int k_L) {
     if (!b || !b->built || !b->d_out) return 2;
     for (ClassPlan& pl : b->plans) {
         if (pl.li != i_L || pl.lj != j_L || pl.lk != k_L) continue;
-        if (!pl.fast || pl.total_items == 0) return 1;
-        cudaMemsetAsync(pl.counter, 0, 2 * sizeof(int), b->stream);
-        int rc = launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, pl.map, pl.total_items, b->omega, b->d_out,
-                               pl.counter, b->stream);
+        if (!pl.fast || (pl.total_items == 0 && pl.total_items32 == 0)) return 1;
+        cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), b->stream);
+        int rc = 0;
+        if (pl.total_items > 0)
+            rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, pl.map, pl.total_items, b->omega, b->d_out,
+                                pl.counter, b->stream);
+        if (pl.total_items32 > 0)
+            rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, pl.map32, pl.total_items32, b->omega, b->d_out,
+                                pl.counter32, b->stream, true);
         return rc == 0 ? 0 : fail(b, "class launch", cudaGetLastError());
     }
+    return 1;
+}
+
+int eip_batch_precision_split(eip_batch* b, int i_L, int j_L, int k_L, long long* triplets_fp64,
+                              long long* triplets_fp32) {
+    if (!b || !b->built) return 2;
+    for (const ClassPlan& pl : b->plans)
+        if (pl.li == i_L && pl.lj == j_L && pl.lk == k_L) {
+            *triplets_fp64 = pl.fast ? pl.triplets64 : 0;
+            *triplets_fp32 = pl.fast ? pl.triplets32 : 0;
+            if (!pl.fast)
+                for (int m = 0; m < b->n_mol; m++) *triplets_fp64 += (long long)pl.n_sp[m] * pl.n_auxsh[m];
+            return 0;
+        }
     return 1;
 }
 
@@ -553,12 +692,12 @@ int eip_batch_status(eip_batch* b) {
     if (!b || !b->built) return 2;
     for (const ClassPlan& pl : b->plans) {
         if (!pl.fast) continue;
-        int st[2] = {0, 0};
+        int st[4] = {0, 0, 0, 0};
         cudaError_t e = cudaMemcpyAsync(st, pl.counter, sizeof(st), cudaMemcpyDeviceToHost, b->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
         if (e != cudaSuccess) return fail(b, "status copy", e);
-        if (st[1] != 0) {
-            snprintf(b->err, sizeof b->err, "class (%d%d|%d) kernel self-check %d", pl.li, pl.lj, pl.lk, st[1]);
+        if (st[1] != 0 || st[3] != 0) {
+            snprintf(b->err, sizeof b->err, "class (%d%d|%d) kernel self-check %d/%d", pl.li, pl.lj, pl.lk, st[1], st[3]);
             return 3;
         }
     }

@@ -229,6 +229,11 @@ struct BraTable {
 // numbered from item_begin[m]; its packed output block starts at element
 // out_begin[m].  checksum (optional) receives the sum of every value written
 // for molecule m.
+//
+// Optional shell-pair list (mixed precision: the FP32 and FP64 kernels of a
+// class each take a subset of the shell pairs): when sp_list is set, molecule
+// m's k-th pair is sp_list[sp_begin[m] + k] (a global index) and its output
+// row is that index minus sp_first[m], the molecule's first pair.
 struct BatchMap {
     int n_mol;
     const int* item_begin;  // n_mol + 1
@@ -236,6 +241,8 @@ struct BatchMap {
     const int* aux_begin;   // n_mol + 1
     const long long* out_begin;
     double* checksum;
+    const int* sp_list;   // optional
+    const int* sp_first;  // n_mol, with sp_list
 };
 
 // One-centre ("ket") table: auxiliary shells of one class (or point charges).

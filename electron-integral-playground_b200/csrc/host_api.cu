@@ -304,7 +304,7 @@ int compute_class(Context& c, int mode, int li, int lj, int lk, bool spherical, 
         cudaMemcpyAsync(misc, host_misc, sizeof(host_misc), cudaMemcpyHostToDevice, c.stream);
         long long* out_begin = reinterpret_cast<long long*>(misc + 16);
         cudaMemsetAsync(out_begin, 0, sizeof(long long), c.stream);
-        BatchMap map{1, misc + 4, misc + 8, misc + 12, out_begin, nullptr};
+        BatchMap map{1, misc + 4, misc + 8, misc + 12, out_begin, nullptr, nullptr, nullptr};
         rc = launch_e_table(li, lj, bra, static_cast<double*>(c.d_etab.ptr), c.stream);
         if (rc == 0) rc = launch_fast3c(li, lj, lk, bra, st.ket, map, (int)items, omega, dout, misc, c.stream);
         c.launches += 2;

@@ -10,8 +10,11 @@ namespace eip {
     int launch_fast3c_##I##J##_v##V(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket, \
                                     const BatchMap& map, int total_items, double omega, double* out,         \
                                     int* counter, cudaStream_t s);
-#define EIP_DECL(I, J)                                                                 \
-    EIP_DECL_V(I, J, 0) EIP_DECL_V(I, J, 1) EIP_DECL_V(I, J, 2) EIP_DECL_V(I, J, 3)    \
+#define EIP_DECL(I, J)                                                                                      \
+    EIP_DECL_V(I, J, 0) EIP_DECL_V(I, J, 1) EIP_DECL_V(I, J, 2) EIP_DECL_V(I, J, 3)                         \
+    int launch_fast3c_##I##J##_f32(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket, \
+                                   const BatchMap& map, int total_items, double omega, double* out,         \
+                                   int* counter, cudaStream_t s);                                           \
     int launch_e_table_##I##J(const BraTable& bra, double* prim_E, cudaStream_t s);
 EIP_DECL(0, 0) EIP_DECL(0, 1) EIP_DECL(1, 1) EIP_DECL(0, 2) EIP_DECL(1, 2) EIP_DECL(2, 2)
 #undef EIP_DECL
@@ -47,17 +50,18 @@ size_t e_table_doubles(int li, int lj) {
 }
 
 int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& ket, const BatchMap& map,
-                  int total_items, double omega, double* out, int* counter, cudaStream_t s) {
+                  int total_items, double omega, double* out, int* counter, cudaStream_t s, bool fp32) {
     if (!fast3c_supported(li, lj, lk)) return 1;
     const double* t = boys_table_device();
-    const int v = g_variant[li * 3 + lj][lk];
+    const int v = fp32 ? 4 : g_variant[li * 3 + lj][lk];
 #define EIP_GO_V(I, J, V) return launch_fast3c_##I##J##_v##V(lk, t, bra, ket, map, total_items, omega, out, counter, s)
-#define EIP_GO(I, J)                  \
-    switch (v) {                      \
-        case 1: EIP_GO_V(I, J, 1);    \
-        case 2: EIP_GO_V(I, J, 2);    \
-        case 3: EIP_GO_V(I, J, 3);    \
-        default: EIP_GO_V(I, J, 0);   \
+#define EIP_GO(I, J)                                                                                          \
+    switch (v) {                                                                                              \
+        case 1: EIP_GO_V(I, J, 1);                                                                            \
+        case 2: EIP_GO_V(I, J, 2);                                                                            \
+        case 3: EIP_GO_V(I, J, 3);                                                                            \
+        case 4: return launch_fast3c_##I##J##_f32(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
+        default: EIP_GO_V(I, J, 0);                                                                           \
     }
     switch (li * 10 + lj) {
         case 0: EIP_GO(0, 0);

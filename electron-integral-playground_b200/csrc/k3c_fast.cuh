@@ -145,14 +145,17 @@ __global__ void e_table_kernel(BraTable bra, double* __restrict__ prim_E) {
     }
 }
 
-template <int LI, int LJ, int LK, int V>
+// T: arithmetic type of the R tetrahedron, ket, bra and accumulation (double,
+// or float for the mixed-precision path).  Boys, R^{(m)}_000, the E^{ij}_t
+// recurrences (precomputed in FP64) and the prefactors are FP64 in both.
+template <int LI, int LJ, int LK, int V, typename T>
 __global__ void __launch_bounds__(Fast3c<LI, LJ, LK, V>::THREADS, Fast3c<LI, LJ, LK, V>::MIN_CTAS)
 k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, BatchMap map, double omega,
          double* __restrict__ out, int* __restrict__ work_counter, int total_items) {
     using C = Fast3c<LI, LJ, LK, V>;
     constexpr int L = C::L;
-    __shared__ double sE[3 * C::NE];
-    __shared__ double sR[C::NR * 32];
+    __shared__ T sE[3 * C::NE];
+    __shared__ T sR[C::NR * 32];
     __shared__ int s_item;
 
     const int lane = threadIdx.x & 31;
@@ -185,9 +188,13 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
         const int n_aux = __ldg(map.aux_begin + m + 1) - aux0;
         const int n_tiles = (n_aux + 31) >> 5;
         const int local = item - __ldg(map.item_begin + m);
-        const int sp_local = local / n_tiles;
-        const int tile = local - sp_local * n_tiles;
-        const int sp = __ldg(map.sp_begin + m) + sp_local;
+        const int sp_k = local / n_tiles;
+        const int tile = local - sp_k * n_tiles;
+        int sp = __ldg(map.sp_begin + m) + sp_k, sp_local = sp_k;
+        if (map.sp_list) {
+            sp = __ldg(map.sp_list + sp);
+            sp_local = sp - __ldg(map.sp_first + m);
+        }
         const int a_local = tile * 32 + lane;
         const bool valid = a_local < n_aux;
         const int a = aux0 + a_local;
@@ -208,33 +215,34 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
             continue;
         }
 
-        double acc[C::NIJ][C::KPW];
+        T acc[C::NIJ][C::KPW];
 #pragma unroll
         for (int i = 0; i < C::NIJ; i++)
 #pragma unroll
-            for (int c = 0; c < C::KPW; c++) acc[i][c] = 0.0;
+            for (int c = 0; c < C::KPW; c++) acc[i][c] = T(0);
 
         for (int pp = pb; pp < pe; pp++) {
             const double4 P = bra.prim_P[pp];
             const double4 PA = bra.prim_PA[pp];
             const double p = P.w;
             for (int e = threadIdx.x; e < 3 * C::NE; e += C::THREADS)
-                sE[e] = __ldg(bra.prim_E + (size_t)pp * 3 * C::NE + e);
+                sE[e] = (T)__ldg(bra.prim_E + (size_t)pp * 3 * C::NE + e);
             for (int kk = 0; kk < nk_max; kk++) {
                 const bool live = kk < nk;
                 const double4 Cq = live ? ket.prim_C[kb + kk] : make_double4(P.x, P.y, P.z, 1.0);
                 const double cc = live ? ket.prim_coef[kb + kk] : 0.0;
                 const double q = Cq.w;
                 const double X = P.x - Cq.x, Y = P.y - Cq.y, Z = P.z - Cq.z;
-                double zeta, pref;
+                double zeta, pref64;
                 if (omega == 0.0) {
                     zeta = p * q / (p + q);
-                    pref = PA.w * cc * kTwoPi52 / (p * q * sqrt(p + q));
+                    pref64 = PA.w * cc * kTwoPi52 / (p * q * sqrt(p + q));
                 } else {
                     zeta = 1.0 / (1.0 / p + 1.0 / q + 1.0 / (omega * omega));
-                    pref = PA.w * cc * kTwoPi52 * omega / (p * q * sqrt(p * q + (p + q) * omega * omega));
+                    pref64 = PA.w * cc * kTwoPi52 * omega / (p * q * sqrt(p * q + (p + q) * omega * omega));
                 }
-                if (LK & 1) pref = -pref;  // (-1)^{|s|} with |s| = LK mod 2
+                if (LK & 1) pref64 = -pref64;  // (-1)^{|s|} with |s| = LK mod 2
+                const T pref = (T)pref64;
 
                 // R^{(m)}_000 = (-2 zeta)^m F_m(zeta |PQ|^2); this warp's share of
                 // the tetrahedron by the closed form (entries are independent).
@@ -249,13 +257,15 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                         g *= f;
                     }
                 }
-                double px[L + 1], py[L + 1], pz[L + 1];
-                px[0] = py[0] = pz[0] = 1.0;
+                T Rt[L + 1], px[L + 1], py[L + 1], pz[L + 1];
+                px[0] = py[0] = pz[0] = T(1);
+#pragma unroll
+                for (int mm = 0; mm <= L; mm++) Rt[mm] = (T)Rm[mm];
 #pragma unroll
                 for (int mm = 1; mm <= L; mm++) {
-                    px[mm] = px[mm - 1] * X;
-                    py[mm] = py[mm - 1] * Y;
-                    pz[mm] = pz[mm - 1] * Z;
+                    px[mm] = px[mm - 1] * (T)X;
+                    py[mm] = py[mm - 1] * (T)Y;
+                    pz[mm] = pz[mm - 1] * (T)Z;
                 }
                 static_for<0, C::KS>([&](auto g) {
                     constexpr int G = decltype(g)::value;
@@ -265,22 +275,22 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                         static_for<lo_e, hi_e>([&](auto e) {
                             constexpr int idx = decltype(e)::value;
                             constexpr int t = herm_t(idx), u = herm_u(idx), v = herm_v(idx);
-                            double r = 0.0;
+                            T r = T(0);
                             static_for<(t + 1) / 2, t + 1>([&](auto mx_) {
                                 constexpr int mx = decltype(mx_)::value;
-                                double ry = 0.0;
+                                T ry = T(0);
                                 static_for<(u + 1) / 2, u + 1>([&](auto my_) {
                                     constexpr int my = decltype(my_)::value;
-                                    double rz = 0.0;
+                                    T rz = T(0);
                                     static_for<(v + 1) / 2, v + 1>([&](auto mz_) {
                                         constexpr int mz = decltype(mz_)::value;
-                                        constexpr double h = hermite_r_coef(v, mz);
-                                        rz = fma(h * pz[2 * mz - v], Rm[mx + my + mz], rz);
+                                        constexpr T h = (T)hermite_r_coef(v, mz);
+                                        rz = fma(h * pz[2 * mz - v], Rt[mx + my + mz], rz);
                                     });
-                                    constexpr double h = hermite_r_coef(u, my);
+                                    constexpr T h = (T)hermite_r_coef(u, my);
                                     ry = fma(h * py[2 * my - u], rz, ry);
                                 });
-                                constexpr double h = hermite_r_coef(t, mx);
+                                constexpr T h = (T)hermite_r_coef(t, mx);
                                 r = fma(h * px[2 * mx - t], ry, r);
                             });
                             sR[idx * 32 + lane] = r;
@@ -288,7 +298,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                     }
                 });
                 // (1/2q)^{LK - j}: weight of the ket terms with |s| = LK - 2j
-                double w[LK / 2 + 1];
+                T w[LK / 2 + 1];
                 {
                     const double inv2q = 0.5 / q;
                     double base = 1.0;
@@ -296,7 +306,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                     for (int j = 0; j < LK - LK / 2; j++) base *= inv2q;
 #pragma unroll
                     for (int j = LK / 2; j >= 0; j--) {
-                        w[j] = base;
+                        w[j] = (T)base;
                         base *= inv2q;
                     }
                 }
@@ -308,11 +318,11 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 // warp, coefficients from constant memory, so the instruction
                 // cache holds one copy.  Either way X[c][h] is formed for all
                 // c first, so each E^{ij}_t shared-memory load feeds KPW FMAs.
-                double Xh[C::KPW][C::NHB];
+                T Xh[C::KPW][C::NHB];
 #pragma unroll
                 for (int c = 0; c < C::KPW; c++)
 #pragma unroll
-                    for (int h = 0; h < C::NHB; h++) Xh[c][h] = 0.0;
+                    for (int h = 0; h < C::NHB; h++) Xh[c][h] = T(0);
                 if constexpr (C::KS == 1) {
                     static_for<0, C::NHB>([&](auto h_) {
                         constexpr int h = decltype(h_)::value;
@@ -320,9 +330,9 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                         static_for<0, LK / 2 + 1>([&](auto j_) {
                             constexpr int j = decltype(j_)::value;
                             constexpr int S = LK - 2 * j;
-                            double part[C::KPW];
+                            T part[C::KPW];
 #pragma unroll
-                            for (int c = 0; c < C::KPW; c++) part[c] = 0.0;
+                            for (int c = 0; c < C::KPW; c++) part[c] = T(0);
                             static_for<0, ncart(S)>([&](auto sc_) {
                                 constexpr int sc = decltype(sc_)::value;
                                 constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
@@ -332,11 +342,11 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                                     return false;
                                 }();
                                 if constexpr (any) {
-                                    const double r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
+                                    const T r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
                                     static_for<0, C::NKO>([&](auto c_) {
                                         constexpr int c = decltype(c_)::value;
                                         constexpr double kc = ket_sph_coef(LK, c, sx, sy, sz);
-                                        if constexpr (kc != 0.0) part[c] = fma(kc, r, part[c]);
+                                        if constexpr (kc != 0.0) part[c] = fma((T)kc, r, part[c]);
                                     });
                                 }
                             });
@@ -352,20 +362,20 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                         static_for<0, ncart(S)>([&](auto sc_) {
                             constexpr int sc = decltype(sc_)::value;
                             constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
-                            double ce[C::KPW];
+                            T ce[C::KPW];
                             bool any = false;
 #pragma unroll
                             for (int c = 0; c < C::KPW; c++) {
                                 const int ko = warp * C::KPW + c;
                                 const double cf = ko < C::NKO ? c_ket_coef<LK>.v[ko][sidx + sc] : 0.0;
-                                ce[c] = cf * w[j];
+                                ce[c] = (T)cf * w[j];
                                 any = any || cf != 0.0;
                             }
                             if (any) {  // warp-uniform
                                 static_for<0, C::NHB>([&](auto h_) {
                                     constexpr int h = decltype(h_)::value;
                                     constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
-                                    const double r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
+                                    const T r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
 #pragma unroll
                                     for (int c = 0; c < C::KPW; c++) Xh[c][h] = fma(ce[c], r, Xh[c][h]);
                                 });
@@ -381,30 +391,30 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                     static_for<0, C::NJ>([&](auto cj_) {
                         constexpr int cj = decltype(cj_)::value;
                         constexpr int jx = cart_x(LJ, cj), jy = cart_y(LJ, cj), jz = cart_z(LJ, cj);
-                        double sxv[C::KPW];
+                        T sxv[C::KPW];
 #pragma unroll
-                        for (int c = 0; c < C::KPW; c++) sxv[c] = 0.0;
+                        for (int c = 0; c < C::KPW; c++) sxv[c] = T(0);
                         static_for<0, ix + jx + 1>([&](auto t_) {
                             constexpr int t = decltype(t_)::value;
-                            double su[C::KPW];
+                            T su[C::KPW];
 #pragma unroll
-                            for (int c = 0; c < C::KPW; c++) su[c] = 0.0;
+                            for (int c = 0; c < C::KPW; c++) su[c] = T(0);
                             static_for<0, iy + jy + 1>([&](auto u_) {
                                 constexpr int u = decltype(u_)::value;
-                                double sv[C::KPW];
+                                T sv[C::KPW];
 #pragma unroll
-                                for (int c = 0; c < C::KPW; c++) sv[c] = 0.0;
+                                for (int c = 0; c < C::KPW; c++) sv[c] = T(0);
                                 static_for<0, iz + jz + 1>([&](auto v_) {
                                     constexpr int v = decltype(v_)::value;
-                                    const double ez = sE[2 * C::NE + e_offset<LJ>(iz, jz) + v];
+                                    const T ez = sE[2 * C::NE + e_offset<LJ>(iz, jz) + v];
 #pragma unroll
                                     for (int c = 0; c < C::KPW; c++) sv[c] = fma(ez, Xh[c][herm_index(t, u, v)], sv[c]);
                                 });
-                                const double ey = sE[C::NE + e_offset<LJ>(iy, jy) + u];
+                                const T ey = sE[C::NE + e_offset<LJ>(iy, jy) + u];
 #pragma unroll
                                 for (int c = 0; c < C::KPW; c++) su[c] = fma(ey, sv[c], su[c]);
                             });
-                            const double ex = sE[e_offset<LJ>(ix, jx) + t];
+                            const T ex = sE[e_offset<LJ>(ix, jx) + t];
 #pragma unroll
                             for (int c = 0; c < C::KPW; c++) sxv[c] = fma(ex, su[c], sxv[c]);
                         });
@@ -428,24 +438,24 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                     constexpr int I = decltype(I_)::value;
                     static_for<0, nsph(LJ)>([&](auto J_) {
                         constexpr int J = decltype(J_)::value;
-                        double v = 0.0;
+                        T v = T(0);
                         static_for<0, C::NI>([&](auto ci_) {
                             constexpr int ci = decltype(ci_)::value;
                             constexpr double wi = sph_coef(LI, I, ci);
                             if constexpr (wi != 0.0) {
-                                double vj = 0.0;
+                                T vj = T(0);
                                 static_for<0, C::NJ>([&](auto cj_) {
                                     constexpr int cj = decltype(cj_)::value;
                                     constexpr double wj = sph_coef(LJ, J, cj);
-                                    if constexpr (wj != 0.0) vj = fma(wj, acc[ci * C::NJ + cj][c], vj);
+                                    if constexpr (wj != 0.0) vj = fma((T)wj, acc[ci * C::NJ + cj][c], vj);
                                 });
-                                v = fma(wi, vj, v);
+                                v = fma((T)wi, vj, v);
                             }
                         });
                         if (valid) {
                             const size_t row = ((size_t)sp_local * C::NIJS + I * nsph(LJ) + J) * C::NKO + ko;
-                            out[obase + row * n_aux + a_local] = v;
-                            wsum += v;
+                            out[obase + row * n_aux + a_local] = (double)v;
+                            wsum += (double)v;
                         }
                     });
                 });
@@ -460,7 +470,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
 }
 
 // Occupancy-sized persistent grid for one class.
-template <int LI, int LJ, int LK, int V>
+template <int LI, int LJ, int LK, int V, typename T>
 static int launch_one(const double* boys_table, const BraTable& bra, const KetTable& ket, const BatchMap& map,
                       int total_items, double omega, double* out, int* counter, cudaStream_t s) {
     using C = Fast3c<LI, LJ, LK, V>;
@@ -468,7 +478,7 @@ static int launch_one(const double* boys_table, const BraTable& bra, const KetTa
     static int max_blocks = 0;
     if (max_blocks == 0) {
         int per_sm = 0, dev = 0, sms = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3c_fast<LI, LJ, LK, V>, C::THREADS, 0) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3c_fast<LI, LJ, LK, V, T>, C::THREADS, 0) !=
             cudaSuccess)
             return 2;
         cudaGetDevice(&dev);
@@ -476,7 +486,8 @@ static int launch_one(const double* boys_table, const BraTable& bra, const KetTa
         max_blocks = (per_sm < 1 ? 1 : per_sm) * sms;
     }
     const int blocks = total_items < max_blocks ? total_items : max_blocks;
-    k3c_fast<LI, LJ, LK, V><<<blocks, C::THREADS, 0, s>>>(boys_table, bra, ket, map, omega, out, counter, total_items);
+    k3c_fast<LI, LJ, LK, V, T><<<blocks, C::THREADS, 0, s>>>(boys_table, bra, ket, map, omega, out, counter,
+                                                             total_items);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 

@@ -7,11 +7,11 @@ int launch_fast3c_00_v0(int lk, const double* boys_table, const BraTable& bra, c
                            const BatchMap& map, int total_items, double omega, double* out, int* counter,
                            cudaStream_t s) {
     switch (lk) {
-        case 0: return launch_one<0, 0, 0, 0>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 1: return launch_one<0, 0, 1, 0>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 2: return launch_one<0, 0, 2, 0>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 3: return launch_one<0, 0, 3, 0>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 4: return launch_one<0, 0, 4, 0>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 0: return launch_one<0, 0, 0, 0, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 1: return launch_one<0, 0, 1, 0, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 2: return launch_one<0, 0, 2, 0, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 3: return launch_one<0, 0, 3, 0, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 4: return launch_one<0, 0, 4, 0, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
     }
     return 1;
 }

@@ -7,11 +7,11 @@ int launch_fast3c_11_v1(int lk, const double* boys_table, const BraTable& bra, c
                            const BatchMap& map, int total_items, double omega, double* out, int* counter,
                            cudaStream_t s) {
     switch (lk) {
-        case 0: return launch_one<1, 1, 0, 1>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 1: return launch_one<1, 1, 1, 1>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 2: return launch_one<1, 1, 2, 1>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 3: return launch_one<1, 1, 3, 1>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 4: return launch_one<1, 1, 4, 1>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 0: return launch_one<1, 1, 0, 1, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 1: return launch_one<1, 1, 1, 1, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 2: return launch_one<1, 1, 2, 1, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 3: return launch_one<1, 1, 3, 1, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 4: return launch_one<1, 1, 4, 1, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
     }
     return 1;
 }

@@ -7,11 +7,11 @@ int launch_fast3c_12_v3(int lk, const double* boys_table, const BraTable& bra, c
                            const BatchMap& map, int total_items, double omega, double* out, int* counter,
                            cudaStream_t s) {
     switch (lk) {
-        case 0: return launch_one<1, 2, 0, 3>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 1: return launch_one<1, 2, 1, 3>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 2: return launch_one<1, 2, 2, 3>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 3: return launch_one<1, 2, 3, 3>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
-        case 4: return launch_one<1, 2, 4, 3>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 0: return launch_one<1, 2, 0, 3, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 1: return launch_one<1, 2, 1, 3, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 2: return launch_one<1, 2, 2, 3, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 3: return launch_one<1, 2, 3, 3, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 4: return launch_one<1, 2, 4, 3, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
     }
     return 1;
 }

@@ -137,7 +137,17 @@ int eip_batch_add_pairs(eip_batch* batch, int molecule, int i_L, int j_L, const 
                         const int* pair_i_ao_start, const int* pair_j_ao_start, int n_pair);
 int eip_batch_add_aux(eip_batch* batch, int molecule, int k_L, const double* aux_A_a,
                       const double* aux_coefficient, const int* aux_i_aux_start, int n_primitive);
+/* Precision of the batch (before build): mode 0 = FP64 everywhere (default);
+ * mode 1 = mixed: a shell pair of a fast class is computed with FP32 R
+ * tetrahedron, ket, bra and accumulation (FP64 Boys, R^m_000, E recurrences
+ * and prefactors) when Q_pair * max Q_aux * (transform gains) < fp32_threshold,
+ * where Q are Schwarz-type upper bounds built like the reference front end's
+ * pair bound; every other shell pair stays FP64. */
+int eip_batch_set_precision(eip_batch* batch, int mode, double fp32_threshold);
 int eip_batch_build(eip_batch* batch);
+/* Contracted triplets of a class computed in FP64 and in FP32 (after build). */
+int eip_batch_precision_split(eip_batch* batch, int i_L, int j_L, int k_L, long long* triplets_fp64,
+                              long long* triplets_fp32);
 long long eip_batch_output_elems(eip_batch* batch);
 int eip_batch_block(eip_batch* batch, int molecule, int i_L, int j_L, int k_L, long long* offset,
                     int* n_pair_shells, int* n_aux_shells);

@@ -94,3 +94,37 @@ def test_every_tuning_variant_matches_reference(small_batch):
         for k, v in saved.items():
             if v >= 0:
                 L.eip_tune_set(*k, v)
+
+
+def _two_fragments():
+    ds = importlib.import_module("electron-integral-playground_b200.data_structure")
+    a = syn.organic_molecule(6, seed=21)
+    b = syn.organic_molecule(6, seed=22)
+    shift = np.array([12.0, 3.0, -2.0]) / 0.52917721054482
+    m = ds.Molecule(elements=a.elements + b.elements, geometry=np.vstack([a.geometry, b.geometry + shift]))
+    syn.attach_synthetic_basis(m, aux_l_max=4, seed=0)
+    return m
+
+
+def test_mixed_precision_within_1e10_of_fp64():
+    m = _two_fragments()
+    pd, ad = pu.form_pair_data(m, 1e-14), pu.form_auxiliary_pair_data(m)
+    f64 = bt.ThreeCenterBatch([m], [pd], [ad], precision="fp64")
+    mix = bt.ThreeCenterBatch([m], [pd], [ad], precision="mixed")
+    f32_triplets = 0
+    for (li, lj) in pd:
+        for lk in ad:
+            split = mix.precision_split(li, lj, lk)
+            if split:
+                f32_triplets += split[1]
+    assert f32_triplets > 0, "the gate should send the far fragment pairs to FP32"
+    for b in (f64, mix):
+        b.alloc_output()
+        b.run()
+        b.status()
+    d64, dmix = f64.dense(0), mix.dense(0)
+    err = np.max(np.abs(d64 - dmix))
+    assert err <= 1e-10, err
+    assert err > 0.0  # the FP32 path really ran
+    f64.close()
+    mix.close()
