@@ -165,6 +165,78 @@ def mixed_error(bt, mols, pds, ads, threshold, torch, budget_bytes=30e9):
     return out
 
 
+def dropin_sample(mols, pds, ads, stats, sample_idx):
+    """The plain FP64 drop-in three_center (reference C ABI, host buffers, dense
+    output) on the GPU over the cpu_baseline's sample molecules."""
+    import importlib
+
+    mi = importlib.import_module("electron-integral-playground_b200.molecular_integral")
+    if not sample_idx:
+        return None
+    mi.three_center(pds[sample_idx[0]], ads[sample_idx[0]], mols[sample_idx[0]])  # warm-up
+    t0 = time.perf_counter()
+    triplets = 0
+    for i in sample_idx:
+        mi.three_center(pds[i], ads[i], mols[i])
+        triplets += sum(d["screened"] for d in stats[i].values())
+    dt = time.perf_counter() - t0
+    return {"value": triplets / dt, "unit": UNIT, "seconds": dt, "molecules": list(sample_idx),
+            "what": "drop-in three_center per class, FP64, dense host output (wall clock incl. copies)"}
+
+
+def run_serving(args, torch, seed):
+    """Open-loop Poisson stream of requests (S, V, (P|Q), (mu nu|P)) of 5-200-atom
+    molecules through the continuous-batching server (mixed precision), and the
+    same requests each served alone in FP64."""
+    import importlib
+
+    import numpy as np
+
+    syn = importlib.import_module("electron-integral-playground_b200.synthetic")
+    pu = importlib.import_module("electron-integral-playground_b200.pair_utility")
+    sv = importlib.import_module("electron-integral-playground_b200.serving")
+    n = args.serve_requests
+    sizes = syn.molecule_sizes(n, 5, 200, seed + 7)
+    rng = np.random.default_rng(seed + 11)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
+    reqs = []
+    for i, (na, t) in enumerate(zip(sizes, arrivals)):
+        m = syn.attach_synthetic_basis(syn.organic_molecule(na, seed * 7919 + i), aux_l_max=4, seed=seed)
+        reqs.append(sv.Request(i, m, pu.form_pair_data(m, 1e-14), pu.form_auxiliary_pair_data(m), float(t)))
+    free, _ = torch.cuda.mem_get_info()
+    budget = min(150e9, free - 12e9)
+    server = sv.IntegralServer(budget_bytes=budget, precision="mixed", fp32_threshold=args.fp32_threshold)
+    warm = sv.Request(-1, reqs[0].molecule, reqs[0].pair_data, reqs[0].aux_data, 0.0)
+    server.serve([warm], realtime=False)
+    server.launches = 0
+    st = server.serve(reqs, realtime=True)
+    pieces = sum(len(server.pieces_of(r)) for r in reqs)
+    del server
+    torch.cuda.empty_cache()
+    alone = []
+    solo = sv.IntegralServer(budget_bytes=budget, precision="fp64", max_inflight=1, host_overlap=False)
+    for r in reqs[:args.serve_alone]:
+        one = sv.Request(r.rid, r.molecule, r.pair_data, r.aux_data, 0.0)
+        alone.append(solo.serve([one], realtime=False)["latency_p50_s"])
+    del solo
+    torch.cuda.empty_cache()
+    lat_alone = np.array(alone)
+    frac = len(alone) / n
+    return {
+        "requests": n, "rate_rps": args.serve_rate, "atoms": [int(x) for x in sizes],
+        "budget_gb": budget / 1e9, "precision": "mixed", "launches": st["launches"], "pieces": pieces,
+        "throughput_rps": st["throughput_rps"], "wall_s": st["wall_s"],
+        "latency_p50_ms": st["latency_p50_s"] * 1e3, "latency_p99_ms": st["latency_p99_s"] * 1e3,
+        "alone_fp64": {"requests": len(alone), "sum_s": float(lat_alone.sum()),
+                       "throughput_rps": len(alone) / float(lat_alone.sum()),
+                       "latency_p50_ms": float(np.percentile(lat_alone, 50)) * 1e3,
+                       "latency_p99_ms": float(np.percentile(lat_alone, 99)) * 1e3,
+                       "note": "each request served alone (nothing else in flight), FP64"
+                               + ("" if frac == 1 else f", first {len(alone)} requests")},
+        "sample": f"{n} of the 10k-request stream (Poisson {args.serve_rate} req/s, 5-200 atoms log-uniform)",
+    }
+
+
 def run_reference_arm(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -204,6 +276,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fp32-threshold", type=float, default=1e-3,
                     help="mixed precision: FP32 for shell pairs with bound below this")
+    ap.add_argument("--serve-requests", type=int, default=24, help="serving sample: requests (0 = skip)")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="serving sample: Poisson arrival rate, req/s")
+    ap.add_argument("--serve-alone", type=int, default=24, help="requests also timed alone in FP64")
     ap.add_argument("--tune", action="store_true",
                     help="run the autotuner on this workload first and rewrite its cache")
     args = ap.parse_args()
@@ -356,12 +431,15 @@ def main():
                 "whole_step_frac_fp64": tot["flops"] / (m64["ms"] * 1e-3) / 1e12 / fp64_peak,
                 "output_store_gbs": tot["out_bytes"] / (head["ms"] * 1e-3) / 1e9}
     cpu = None
+    dropin = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         smp = reference_sample(mols, pds, ads, stats, args.ref_budget)
         if smp is not None:
             cpu = {"value": smp["value"], "unit": UNIT, "cores": smp["cores"], "kind": "reference",
                    "sample": f"molecules {smp['molecules']} of the batch (dense output <= 2e8 doubles each), "
                              f"{smp['triplets']} screened triplets, {smp['seconds']:.1f} s"}
+            dropin = dropin_sample(mols, pds, ads, stats, smp["molecules"])
+    serving = run_serving(args, torch, args.seed + 1000 * rank) if args.serve_requests > 0 else None
     if rank == 0:
         per = head["per_step"]
         line = {
@@ -390,9 +468,10 @@ def main():
                     "wall_ms_per_step": head["e2e_wall_ms"],
                     "fp64_value": screened / (m64["e2e_ms"] * 1e-3),
                     "result": "per-molecule checksum of the packed (mu nu|P) (computed in the kernels' epilogue)"},
-            "roofline": roof, "cpu_baseline": cpu,
+            "roofline": roof, "cpu_baseline": cpu, "dropin_fp64": dropin, "serving": serving,
             "gpu_launches": head["launches"], "clocks": head["clocks"], "clocks_fp64": m64["clocks"],
-            "latency_ms": {"p50": statistics.median(per), "p99": sorted(per)[min(len(per) - 1, int(0.99 * len(per)))]},
+            "latency_ms": {"p50": statistics.median(per), "p99": sorted(per)[min(len(per) - 1, int(0.99 * len(per)))],
+                           "what": "per-step (whole batch) device time; request latency is under serving"},
             "class_ms": {f"{k[0]}{k[1]}|{k[2]}": round(v, 4) for k, v in sorted(class_ms.items())},
             "tuning": "autotuned variants (tuning/b200_fp64.json)" if tuning else "default variants",
         }

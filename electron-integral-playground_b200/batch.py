@@ -6,6 +6,17 @@ device; every run is one CUDA-graph launch that computes every
 (one block per molecule and class, layout [pair shell][I][J][K][aux shell]).
 ``dense(m)`` expands molecule m's blocks into the reference's dense
 (n_aux, n_ao, n_ao) layout (used by tests; the packed form is the product).
+
+Two more integral kinds run through the same kernels:
+
+* nuclear attraction V[mu nu C]: point charges per molecule (``charges_list``)
+  form the ket class ``POINT_CHARGES`` (l_k = 0, one block entry per charge);
+  ``dense_V(m)`` gives the reference's (n_ao, n_ao, n_charge) layout;
+* the two-centre metric (P|Q): ``metric_pair_tables(aux)`` turns the auxiliary
+  basis into one-centre pair tables (an exponent-0 s function times each
+  auxiliary primitive, A = B = P), so a molecule slot with those pairs and the
+  auxiliary tables as ket computes (0, l_P | l_Q) blocks; ``dense_metric(m)``
+  gives the reference's (n_aux, n_aux) layout.
 """
 
 import ctypes
@@ -15,6 +26,27 @@ import numpy as np
 from ._lib import IntegralError, as_f64, as_i32, dp, ip, lib
 
 _vp = ctypes.c_void_p
+
+POINT_CHARGES = -1  # ket-class key of point charges (EIP_POINT_CHARGES)
+
+
+def metric_pair_tables(aux_data):
+    """(P|Q) as three-centre classes (0, l_P | l_Q): every auxiliary primitive
+    becomes a one-centre pair: A = (P, exponent 0), B = (P, q), P_p = (P, q),
+    coefficient = the primitive's, i_ao_start = 0, j_ao_start = P's first
+    function."""
+    from .data_structure import PrimitivePairData
+
+    out = {}
+    for l, a in aux_data.items():
+        B = np.ascontiguousarray(np.asarray(a.A_a, np.float64))
+        A = B.copy()
+        A[:, 3] = 0.0
+        st = np.asarray(a.i_ao_start, np.int32)
+        out[(0, int(l))] = PrimitivePairData(P_p=B, A_a=A, B_b=B, coefficient=np.ascontiguousarray(a.coefficient),
+                                             i_ao_start=np.zeros_like(st), j_ao_start=st.copy(), i_atom=None,
+                                             j_atom=None)
+    return out
 
 
 def _bind(L):
@@ -27,6 +59,7 @@ def _bind(L):
     L.eip_batch_create.restype = _vp
     L.eip_batch_add_pairs.argtypes = [_vp, c_int, c_int, c_int, _dpp, _dpp, _dpp, _dpp, _ipp, _ipp, c_int]
     L.eip_batch_add_aux.argtypes = [_vp, c_int, c_int, _dpp, _dpp, _ipp, c_int]
+    L.eip_batch_add_charges.argtypes = [_vp, c_int, _dpp, c_int]
     L.eip_batch_build.argtypes = [_vp]
     L.eip_batch_set_precision.argtypes = [_vp, c_int, c_double]
     L.eip_batch_precision_split.argtypes = [_vp, c_int, c_int, c_int, ctypes.POINTER(c_ll), ctypes.POINTER(c_ll)]
@@ -66,9 +99,13 @@ class ThreeCenterBatch:
     fp32_threshold; FP64 Boys, E recurrences, prefactors and every other pair)."""
 
     def __init__(self, molecules, pair_data_list, aux_data_list, omega: float = 0.0, precision: str = "fp64",
-                 fp32_threshold: float = DEFAULT_FP32_THRESHOLD):
+                 fp32_threshold: float = DEFAULT_FP32_THRESHOLD, charges_list=None):
         if not (len(molecules) == len(pair_data_list) == len(aux_data_list)) or not molecules:
             raise ValueError("need one pair table and one auxiliary table per molecule")
+        if charges_list is None:
+            charges_list = [None] * len(molecules)
+        if len(charges_list) != len(molecules):
+            raise ValueError("need one charge array (or None) per molecule")
         spherical = {bool(m.spherical_basis) for m in molecules}
         if len(spherical) != 1:
             raise ValueError("all molecules of a batch must share spherical_basis")
@@ -77,6 +114,7 @@ class ThreeCenterBatch:
         self.molecules = molecules
         self.pair_data_list = pair_data_list
         self.aux_data_list = aux_data_list
+        self.charges_list = charges_list
         self.spherical = spherical.pop()
         self.omega = float(omega)
         self.h = self.L.eip_batch_create(len(molecules), self.spherical, self.omega)
@@ -101,6 +139,10 @@ class ThreeCenterBatch:
                 self._keep.append(arrs)
                 self._check(self.L.eip_batch_add_aux(self.h, m, int(lk), dp(arrs[0]), dp(arrs[1]), ip(arrs[2]),
                                                      arrs[0].shape[0]), "add_aux")
+            if charges_list[m] is not None and len(charges_list[m]) > 0:
+                c = as_f64(np.asarray(charges_list[m]).reshape(-1, 3), (3,))
+                self._keep.append([c])
+                self._check(self.L.eip_batch_add_charges(self.h, m, dp(c), c.shape[0]), "add_charges")
         self._check(self.L.eip_batch_build(self.h), "build")
         self._keep = None
         self.output_elems = int(self.L.eip_batch_output_elems(self.h))
@@ -204,6 +246,51 @@ class ThreeCenterBatch:
                 off_diag = np.broadcast_to((pairs[:, 0] != pairs[:, 1])[:, None, None, None, None], buf.shape)
                 J[K[off_diag], Jc[off_diag], I[off_diag]] = buf[off_diag]
         return J
+
+    def _block_array(self, m, li, lj, lk, ni, nj, nk):
+        blk = self.block(m, li, lj, lk)
+        if blk is None or blk[1] == 0 or blk[2] == 0:
+            return None
+        off, nsp, nax = blk
+        buf = np.empty(nsp * ni * nj * nk * nax)
+        self._check(self.L.eip_batch_copy_output(self.h, off, buf.size, dp(buf)), "copy_output")
+        return buf.reshape(nsp, ni, nj, nk, nax)
+
+    def dense_V(self, m):
+        """Molecule m's V[mu nu C] in the reference's layout (n_ao, n_ao, n_charge)."""
+        mol = self.molecules[m]
+        nc = len(self.charges_list[m])
+        V = np.zeros((mol.n_ao, mol.n_ao, nc))
+        n_of = (lambda l: 2 * l + 1) if self.spherical else (lambda l: (l + 1) * (l + 2) // 2)
+        for (li, lj), p in self.pair_data_list[m].items():
+            ni, nj = n_of(li), n_of(lj)
+            buf = self._block_array(m, li, lj, POINT_CHARGES, ni, nj, 1)
+            if buf is None:
+                continue
+            pairs = np.unique(np.stack([np.asarray(p.i_ao_start), np.asarray(p.j_ao_start)], 1), axis=0)
+            for s, (i0, j0) in enumerate(pairs):
+                V[i0:i0 + ni, j0:j0 + nj, :] = buf[s, :, :, 0, :]
+                if i0 != j0:
+                    V[j0:j0 + nj, i0:i0 + ni, :] = buf[s, :, :, 0, :].transpose(1, 0, 2)
+        return V
+
+    def dense_metric(self, m):
+        """(P|Q) of a slot built from metric_pair_tables: (n_aux, n_aux)."""
+        mol = self.molecules[m]
+        M = np.zeros((mol.n_aux, mol.n_aux))
+        n_of = (lambda l: 2 * l + 1) if self.spherical else (lambda l: (l + 1) * (l + 2) // 2)
+        for (li, lj), p in self.pair_data_list[m].items():
+            p_starts = np.unique(np.asarray(p.j_ao_start))
+            for lk, a in self.aux_data_list[m].items():
+                nj, nk = n_of(lj), n_of(lk)
+                buf = self._block_array(m, li, lj, lk, 1, nj, nk)
+                if buf is None:
+                    continue
+                q_starts = np.unique(np.asarray(a.i_ao_start))
+                for s, p0 in enumerate(p_starts):
+                    for t, q0 in enumerate(q_starts):
+                        M[p0:p0 + nj, q0:q0 + nk] = buf[s, 0, :, :, t]
+        return M
 
     def close(self):
         if self.h:

@@ -11,6 +11,9 @@
 //   overlap.
 // Classes outside the fast kernels' range run as generic raw + transform
 // kernels, one pair per molecule, inside the same graph.
+// Point charges (eip_batch_add_charges) form one more ket class, key
+// kPointKet: the nuclear-attraction integrals V[mu nu C] of unit charges, run
+// by the same kernels with a point-charge ket (l_k = 0, one block per charge).
 // Output: one packed block per (molecule, class), offsets from
 // eip_batch_block(); see k3c_fast.cuh for the layout.
 #include <stdio.h>
@@ -37,8 +40,12 @@ struct AuxIn {
     std::vector<int> start;
 };
 
+// Ket-class key of point charges in the per-molecule auxiliary maps.
+constexpr int kPointKet = EIP_POINT_CHARGES;
+
 struct ClassPlan {
-    int li, lj, lk;
+    int li, lj, lk;     // lk = kPointKet for point charges
+    bool point = false;
     bool fast;
     int total_items = 0;
     BraTable bra{};
@@ -146,7 +153,13 @@ void group_indices(const int* ia, const int* ja, int n, std::vector<int>& order,
 // distance shift applied once: 2 |c_a c_b| (la/2ea)^(la/2) (lb/2eb)^(lb/2)
 // exp(-ab/p d^2) max((pi/p)^1.5, 2^0.25 (pi/p)^1.25), d = max(|AB| - sqrt(la/2a)
 // - sqrt(lb/2b), 0); |c_a c_b| recovered from c_ab = c_a c_b exp(-ab/p |AB|^2).
+double aux_bound(double q, double coef, int l);
+
 double pair_bound(const double* A, const double* B, double coef, int la, int lb) {
+    // A one-centre "pair" (an s function of exponent 0 times one Gaussian: the
+    // bra of the two-centre metric run as a three-centre class) is bounded
+    // like an auxiliary function.
+    if (A[3] == 0.0 && la == 0) return aux_bound(B[3], coef, lb);
     const double a = A[3], b = B[3], p = a + b, mu = a * b / p;
     const double dx = A[0] - B[0], dy = A[1] - B[1], dz = A[2] - B[2];
     const double ab2 = dx * dx + dy * dy + dz * dz, ab = sqrt(ab2);
@@ -225,6 +238,18 @@ int eip_batch_add_aux(eip_batch* b, int mol, int k_L, const double* A_a, const d
     a.C.insert(a.C.end(), A_a, A_a + 4 * (size_t)n_primitive);
     a.coef.insert(a.coef.end(), coefficient, coefficient + n_primitive);
     a.start.insert(a.start.end(), aux_start, aux_start + n_primitive);
+    return 0;
+}
+
+int eip_batch_add_charges(eip_batch* b, int mol, const double* position, int n_charge) {
+    if (!b || b->built || mol < 0 || mol >= b->n_mol || n_charge < 0) return 2;
+    AuxIn& a = b->aux[mol][kPointKet];
+    const int first = (int)a.start.size();
+    for (int c = 0; c < n_charge; c++) {
+        a.C.insert(a.C.end(), {position[3 * (size_t)c], position[3 * (size_t)c + 1], position[3 * (size_t)c + 2], 1.0});
+        a.coef.push_back(1.0);
+        a.start.push_back(first + c);
+    }
     return 0;
 }
 
@@ -308,7 +333,8 @@ int eip_batch_build(eip_batch* b) {
                     H.start.push_back(gi[g]);
                     H.begin.push_back(prim0 + gb[g + 1]);
                     double qa = 0.0;
-                    for (int k = gb[g]; k < gb[g + 1]; k++) qa += aux_bound(a.C[4 * order[k] + 3], a.coef[order[k]], ac.first);
+                    for (int k = gb[g]; k < gb[g + 1]; k++)
+                        if (ac.first != kPointKet) qa += aux_bound(a.C[4 * order[k] + 3], a.coef[order[k]], ac.first);
                     qmax = fmax(qmax, qa);
                 }
                 for (int k = 0; k < n; k++) {
@@ -328,11 +354,13 @@ int eip_batch_build(eip_batch* b) {
             pl.li = pc.first.first;
             pl.lj = pc.first.second;
             pl.lk = ac.first;
-            pl.fast = b->spherical && fast3c_supported(pl.li, pl.lj, pl.lk);
+            pl.point = ac.first == kPointKet;
+            const int lk = pl.point ? 0 : pl.lk;
+            pl.fast = b->spherical && fast3c_supported(pl.li, pl.lj, lk);
             const BraHost& B = bh[pc.first];
             const KetHost& K = kh[ac.first];
             const int ni = b->spherical ? nsph(pl.li) : ncart(pl.li), nj = b->spherical ? nsph(pl.lj) : ncart(pl.lj),
-                      nk = b->spherical ? nsph(pl.lk) : ncart(pl.lk);
+                      nk = b->spherical ? nsph(lk) : ncart(lk);
             long long items = 0;
             for (int m = 0; m < b->n_mol; m++) {
                 const int nsp = B.sp_begin[m + 1] - B.sp_begin[m], nax = K.aux_begin[m + 1] - K.aux_begin[m];
@@ -347,11 +375,11 @@ int eip_batch_build(eip_batch* b) {
                 items += (long long)nsp * ((nax + 31) / 32);
                 if (!pl.fast)
                     b->scratch_elems = std::max(b->scratch_elems, (size_t)nsp * nax * ncart(pl.li) * ncart(pl.lj) *
-                                                                      ncart(pl.lk));
+                                                                      ncart(lk));
             }
             if (items > 0x7fffffffLL) return fail(b, "too many work items in one class", cudaSuccess);
             pl.total_items = (int)items;
-            pl.flops_weight = (double)pl.out_elems * (pl.li + pl.lj + pl.lk + 1);
+            pl.flops_weight = (double)pl.out_elems * (pl.li + pl.lj + lk + 1);
             b->plans.push_back(pl);
         }
     // ---- one pinned buffer with every table, mirrored on the device
@@ -382,9 +410,9 @@ int eip_batch_build(eip_batch* b) {
         ClassPlan& pl = b->plans[i];
         const BraHost& B = bh[{pl.li, pl.lj}];
         const KetHost& K = kh[pl.lk];
-        const bool mixed = b->precision == 1 && pl.fast;
+        const bool mixed = b->precision == 1 && pl.fast && !pl.point;
         const double gain = transform_gain(pl.li, b->spherical) * transform_gain(pl.lj, b->spherical) *
-                            transform_gain(pl.lk, b->spherical);
+                            transform_gain(pl.point ? 0 : pl.lk, b->spherical);
         std::vector<int>& v = plan_ints[i];
         v.assign(6 * (nm + 1) + 4, 0);
         int* ib64 = &v[0];
@@ -476,7 +504,7 @@ int eip_batch_build(eip_batch* b) {
         memcpy(at<long long>(h, plan_ob[i]), pl.out_begin.data(), sizeof(long long) * nm);
         int* dp = at<int>(d, plan_off[i]);
         const long long* dob = at<long long>(d, plan_ob[i]);
-        const bool mixed = b->precision == 1 && pl.fast;
+        const bool mixed = b->precision == 1 && pl.fast && !pl.point;
         int* counters = dp + 6 * (nm + 1);
         const int* list64 = counters + 4;
         const int* list32 = list64 + (v.size() - 6 * (nm + 1) - 4) - pl.n_sp_total32;
@@ -582,8 +610,10 @@ static int capture(eip_batch* b, bool checksum) {
             if (pl.total_items > 0) {
                 BatchMap map = pl.map;
                 map.checksum = checksum ? b->d_checksum : nullptr;
-                rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, map, pl.total_items, b->omega, b->d_out,
-                                    pl.counter, s);
+                rc |= pl.point ? launch_fast_point(pl.li, pl.lj, pl.bra, pl.ket, map, pl.total_items, b->omega,
+                                                   b->d_out, pl.counter, s)
+                               : launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, map, pl.total_items, b->omega,
+                                               b->d_out, pl.counter, s);
                 launches++;
             }
             if (pl.total_items32 > 0) {
@@ -605,8 +635,9 @@ static int capture(eip_batch* b, bool checksum) {
                 ket.n_group = pl.n_auxsh[m];
                 ket.grp_begin += pl.aux0[m];
                 ket.grp_start += pl.aux0[m];
-                rc |= launch_generic_raw(0, pl.li, pl.lj, pl.lk, bra, ket, b->omega, 0, b->d_scratch, s);
-                rc |= launch_transform(pl.li, pl.lj, pl.lk, b->spherical, pl.n_sp[m], pl.n_auxsh[m], b->d_scratch,
+                const int lk = pl.point ? 0 : pl.lk;
+                rc |= launch_generic_raw(pl.point ? 1 : 0, pl.li, pl.lj, lk, bra, ket, b->omega, 0, b->d_scratch, s);
+                rc |= launch_transform(pl.li, pl.lj, lk, b->spherical, pl.n_sp[m], pl.n_auxsh[m], b->d_scratch,
                                        b->d_out + pl.out_begin[m], s);
                 launches += 2;
             }
@@ -641,8 +672,10 @@ int eip_batch_run_class(eip_batch* b, int i_L, int j_L, int k_L) {
         cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), b->stream);
         int rc = 0;
         if (pl.total_items > 0)
-            rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, pl.map, pl.total_items, b->omega, b->d_out,
-                                pl.counter, b->stream);
+            rc |= pl.point ? launch_fast_point(pl.li, pl.lj, pl.bra, pl.ket, pl.map, pl.total_items, b->omega,
+                                               b->d_out, pl.counter, b->stream)
+                           : launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, pl.map, pl.total_items, b->omega,
+                                           b->d_out, pl.counter, b->stream);
         if (pl.total_items32 > 0)
             rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, pl.map32, pl.total_items32, b->omega, b->d_out,
                                 pl.counter32, b->stream, true);

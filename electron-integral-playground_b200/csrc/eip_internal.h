@@ -20,6 +20,8 @@ int fast3c_variant(int li, int lj, int lk);
 int fast3c_set_variant(int li, int lj, int lk, int v);
 size_t e_table_doubles(int li, int lj);
 int launch_e_table(int li, int lj, const BraTable& bra, double* prim_E, cudaStream_t s);
+int launch_fast_point(int li, int lj, const BraTable& bra, const KetTable& ket, const BatchMap& map,
+                      int total_items, double omega, double* out, int* counter, cudaStream_t s);
 int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& ket, const BatchMap& map,
                   int total_items, double omega, double* out, int* counter, cudaStream_t s, bool fp32 = false);
 

@@ -16,29 +16,28 @@ namespace eip {
                                    const BatchMap& map, int total_items, double omega, double* out,         \
                                    int* counter, cudaStream_t s);                                           \
     int launch_e_table_##I##J(const BraTable& bra, double* prim_E, cudaStream_t s);
-EIP_DECL(0, 0) EIP_DECL(0, 1) EIP_DECL(1, 1) EIP_DECL(0, 2) EIP_DECL(1, 2) EIP_DECL(2, 2)
+EIP_DECL(0, 0) EIP_DECL(0, 1) EIP_DECL(1, 1) EIP_DECL(0, 2) EIP_DECL(1, 2) EIP_DECL(2, 2) EIP_DECL(0, 3) EIP_DECL(0, 4)
 #undef EIP_DECL
 #undef EIP_DECL_V
 
-// Variant per (l_i, l_j, l_k): index li*3+lj (li <= lj <= 2), lk.  Defaults from
-// the autotuner's run on B200 (tuning/b200_fp64.json); eip_tune_set overrides.
-static int g_variant[9][5] = {
-    {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0},
-    {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0},
-    {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0},
-};
+// Fast pair classes: l_i <= l_j <= 2 (orbital shell pairs) and (0, 3), (0, 4)
+// (a one-centre bra: the two-centre metric (P|Q) as pair class (0, l_P) with
+// A = B = P).  Variant per (l_i, l_j, l_k), default 0; the autotuner's choices
+// on B200 (tuning/b200_fp64.json) are applied with eip_tune_set.
+static int g_variant[5][5][5] = {};
 
 bool fast3c_supported(int li, int lj, int lk) {
-    return li >= 0 && li <= lj && lj <= 2 && lk >= 0 && lk <= 4;
+    const bool pair_ok = li >= 0 && li <= lj && (lj <= 2 || (li == 0 && lj <= 4));
+    return pair_ok && lk >= 0 && lk <= 4;
 }
 
 int fast3c_variant(int li, int lj, int lk) {
-    return fast3c_supported(li, lj, lk) ? g_variant[li * 3 + lj][lk] : -1;
+    return fast3c_supported(li, lj, lk) ? g_variant[li][lj][lk] : -1;
 }
 
 int fast3c_set_variant(int li, int lj, int lk, int v) {
     if (!fast3c_supported(li, lj, lk) || v < 0 || v > 3) return 1;
-    g_variant[li * 3 + lj][lk] = v;
+    g_variant[li][lj][lk] = v;
     return 0;
 }
 
@@ -53,7 +52,7 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
                   int total_items, double omega, double* out, int* counter, cudaStream_t s, bool fp32) {
     if (!fast3c_supported(li, lj, lk)) return 1;
     const double* t = boys_table_device();
-    const int v = fp32 ? 4 : g_variant[li * 3 + lj][lk];
+    const int v = fp32 ? 4 : g_variant[li][lj][lk];
 #define EIP_GO_V(I, J, V) return launch_fast3c_##I##J##_v##V(lk, t, bra, ket, map, total_items, omega, out, counter, s)
 #define EIP_GO(I, J)                                                                                          \
     switch (v) {                                                                                              \
@@ -70,6 +69,8 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
         case 2: EIP_GO(0, 2);
         case 12: EIP_GO(1, 2);
         case 22: EIP_GO(2, 2);
+        case 3: EIP_GO(0, 3);
+        case 4: EIP_GO(0, 4);
     }
 #undef EIP_GO
 #undef EIP_GO_V
@@ -84,6 +85,8 @@ int launch_e_table(int li, int lj, const BraTable& bra, double* prim_E, cudaStre
         case 2: return launch_e_table_02(bra, prim_E, s);
         case 12: return launch_e_table_12(bra, prim_E, s);
         case 22: return launch_e_table_22(bra, prim_E, s);
+        case 3: return launch_e_table_03(bra, prim_E, s);
+        case 4: return launch_e_table_04(bra, prim_E, s);
     }
     return 1;
 }

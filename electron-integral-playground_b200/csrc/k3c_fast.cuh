@@ -148,7 +148,11 @@ __global__ void e_table_kernel(BraTable bra, double* __restrict__ prim_E) {
 // T: arithmetic type of the R tetrahedron, ket, bra and accumulation (double,
 // or float for the mixed-precision path).  Boys, R^{(m)}_000, the E^{ij}_t
 // recurrences (precomputed in FP64) and the prefactors are FP64 in both.
-template <int LI, int LJ, int LK, int V, typename T>
+// POINT: the ket is a unit point charge instead of an auxiliary Gaussian (the
+// nuclear-attraction integral V[mu nu C], MI/nuclear_attraction.cpp:23-114):
+// zeta = p (omega > 0: p w^2 / (p + w^2)), prefactor c_ab 2 pi / p
+// (omega > 0: c_ab 2 pi w / (p sqrt(p + w^2))), l_k = 0.
+template <int LI, int LJ, int LK, int V, typename T, bool POINT = false>
 __global__ void __launch_bounds__(Fast3c<LI, LJ, LK, V>::THREADS, Fast3c<LI, LJ, LK, V>::MIN_CTAS)
 k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, BatchMap map, double omega,
          double* __restrict__ out, int* __restrict__ work_counter, int total_items) {
@@ -234,7 +238,16 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 const double q = Cq.w;
                 const double X = P.x - Cq.x, Y = P.y - Cq.y, Z = P.z - Cq.z;
                 double zeta, pref64;
-                if (omega == 0.0) {
+                if constexpr (POINT) {
+                    static_assert(LK == 0, "point charges have no angular momentum");
+                    if (omega == 0.0) {
+                        zeta = p;
+                        pref64 = PA.w * cc * 2.0 * kPi / p;
+                    } else {
+                        zeta = p * omega * omega / (p + omega * omega);
+                        pref64 = PA.w * cc * 2.0 * kPi * omega / (p * sqrt(p + omega * omega));
+                    }
+                } else if (omega == 0.0) {
                     zeta = p * q / (p + q);
                     pref64 = PA.w * cc * kTwoPi52 / (p * q * sqrt(p + q));
                 } else {
@@ -470,7 +483,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
 }
 
 // Occupancy-sized persistent grid for one class.
-template <int LI, int LJ, int LK, int V, typename T>
+template <int LI, int LJ, int LK, int V, typename T, bool POINT = false>
 static int launch_one(const double* boys_table, const BraTable& bra, const KetTable& ket, const BatchMap& map,
                       int total_items, double omega, double* out, int* counter, cudaStream_t s) {
     using C = Fast3c<LI, LJ, LK, V>;
@@ -478,7 +491,7 @@ static int launch_one(const double* boys_table, const BraTable& bra, const KetTa
     static int max_blocks = 0;
     if (max_blocks == 0) {
         int per_sm = 0, dev = 0, sms = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3c_fast<LI, LJ, LK, V, T>, C::THREADS, 0) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3c_fast<LI, LJ, LK, V, T, POINT>, C::THREADS, 0) !=
             cudaSuccess)
             return 2;
         cudaGetDevice(&dev);
@@ -486,8 +499,8 @@ static int launch_one(const double* boys_table, const BraTable& bra, const KetTa
         max_blocks = (per_sm < 1 ? 1 : per_sm) * sms;
     }
     const int blocks = total_items < max_blocks ? total_items : max_blocks;
-    k3c_fast<LI, LJ, LK, V, T><<<blocks, C::THREADS, 0, s>>>(boys_table, bra, ket, map, omega, out, counter,
-                                                             total_items);
+    k3c_fast<LI, LJ, LK, V, T, POINT><<<blocks, C::THREADS, 0, s>>>(boys_table, bra, ket, map, omega, out,
+                                                                    counter, total_items);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 

@@ -1,0 +1,320 @@
+"""Continuous-batching integral server (device-resident request loop).
+
+A request is one molecule (its pair and auxiliary tables, the C-ABI formats)
+asking for S, V, (P|Q) and (mu nu|P).  The server
+
+* splits each request into device pieces: (mu nu|P) in slices of auxiliary
+  shells small enough for the HBM budget (a 200-atom molecule's packed
+  (mu nu|P) alone is ~650 GB), (P|Q) (the one-centre metric as pair classes
+  (0, l_P), `batch.metric_pair_tables`), and V (the pair tables with the
+  nuclei as point-charge ket);
+* admits pieces in arrival order whenever the device arena (one allocation of
+  `budget_bytes`, first-fit sub-allocated) has room for their packed output,
+  so requests that arrive while others run are admitted as memory frees up;
+* batches every piece admitted at one moment into ONE batch (one CUDA-graph
+  launch over all their classes) on its own stream; up to `max_inflight`
+  launches overlap on the device;
+* when a launch completes, hands each of its pieces' packed class blocks
+  (device views into the arena) to `consumer(request, piece, blocks)` (default:
+  a per-request digest, sum of squares, on the device) and frees the launch's
+  arena range; S comes from the drop-in overlap entry point on a worker thread
+  while the GPU works.
+
+Latency of a request = completion of its last piece minus its arrival.
+Precision "mixed" uses the batch's FP32 gate (<= 1e-10 of FP64, tested);
+V is always FP64.
+"""
+
+import collections
+import queue
+import threading
+import time
+
+import numpy as np
+
+from .batch import POINT_CHARGES, ThreeCenterBatch, metric_pair_tables
+
+_Z = {"H": 1.0, "He": 2.0, "C": 6.0, "N": 7.0, "O": 8.0, "F": 9.0}
+
+
+def aux_slices(aux_data, n_aux, max_functions):
+    """Split the auxiliary tables into slices of whole shells, at most
+    max_functions functions each (one shell at least), starts rebased to the
+    slice.  Returns [(first function, end function, tables)]."""
+    from .data_structure import PrimitivePairData
+
+    starts = np.unique(np.concatenate([np.asarray(a.i_ao_start) for a in aux_data.values()]))
+    edges = [0]
+    for s in starts:
+        if s - edges[-1] >= max_functions:
+            edges.append(int(s))
+    edges.append(n_aux)
+    slices = []
+    for lo, hi in zip(edges[:-1], edges[1:]):
+        sub = {}
+        for l, a in aux_data.items():
+            st = np.asarray(a.i_ao_start)
+            sel = (st >= lo) & (st < hi)
+            if sel.any():
+                sub[l] = PrimitivePairData(P_p=None, A_a=np.ascontiguousarray(np.asarray(a.A_a)[sel]), B_b=None,
+                                           coefficient=np.ascontiguousarray(np.asarray(a.coefficient)[sel]),
+                                           i_ao_start=(st[sel] - lo).astype(np.int32), j_ao_start=None,
+                                           i_atom=None, j_atom=None)
+        if sub:
+            slices.append((lo, hi, sub))
+    return slices
+
+
+def _n_shell_pairs(p):
+    key = np.asarray(p.i_ao_start).astype(np.int64) * (1 << 32) + np.asarray(p.j_ao_start)
+    return len(np.unique(key))
+
+
+def packed_elems(pair_data, aux_data, n_charge=0):
+    """Doubles of the packed spherical output of one molecule slot."""
+    total = 0
+    n_aux_sh = {l: len(np.unique(np.asarray(a.i_ao_start))) for l, a in aux_data.items()}
+    for (li, lj), p in pair_data.items():
+        n_sp = _n_shell_pairs(p)
+        for lk, nax in n_aux_sh.items():
+            total += n_sp * (2 * li + 1) * (2 * lj + 1) * (2 * lk + 1) * nax
+        total += n_sp * (2 * li + 1) * (2 * lj + 1) * n_charge
+    return total
+
+
+class Request:
+    def __init__(self, rid, molecule, pair_data, aux_data, arrival=0.0):
+        self.rid = rid
+        self.molecule = molecule
+        self.pair_data = pair_data
+        self.aux_data = aux_data
+        self.arrival = arrival
+        self.pieces_left = 0
+        self.digest = 0.0
+        self.done = None
+        self.S = None
+
+
+class Piece:
+    """One molecule slot of a batch: kind "3c" (an auxiliary slice starting at
+    function aux_lo), "metric" (rows of (P|Q) from aux_lo) or "V"."""
+
+    def __init__(self, request, kind, pair_data, aux_data, aux_lo, elems, charges=None):
+        self.request = request
+        self.kind = kind
+        self.pair_data = pair_data
+        self.aux_data = aux_data
+        self.aux_lo = aux_lo
+        self.elems = elems
+        self.charges = charges
+
+    def classes(self):
+        for (li, lj) in self.pair_data:
+            for lk in self.aux_data:
+                yield li, lj, lk
+            if self.charges is not None:
+                yield li, lj, POINT_CHARGES
+
+
+class Arena:
+    """First-fit sub-allocator over one device buffer (offsets in doubles,
+    256-byte granules)."""
+
+    def __init__(self, torch, n_doubles):
+        self.buf = torch.empty(int(n_doubles), dtype=torch.float64, device="cuda")
+        self.free = [(0, int(n_doubles))]
+
+    def alloc(self, n):
+        n = (int(n) + 31) & ~31
+        for i, (off, size) in enumerate(self.free):
+            if size >= n:
+                self.free[i] = (off + n, size - n)
+                if self.free[i][1] == 0:
+                    self.free.pop(i)
+                return off, n
+        return None
+
+    def release(self, off, n):
+        self.free.append((off, n))
+        self.free.sort()
+        merged = []
+        for o, s in self.free:
+            if merged and merged[-1][0] + merged[-1][1] == o:
+                merged[-1] = (merged[-1][0], merged[-1][1] + s)
+            else:
+                merged.append((o, s))
+        self.free = merged
+
+    @property
+    def largest_free(self):
+        return max((s for _, s in self.free), default=0)
+
+    @property
+    def capacity(self):
+        return self.buf.numel()
+
+
+def default_consumer(request, piece, blocks):
+    """blocks: [((l_i, l_j, l_k), device view of the packed block)] of one piece."""
+    for _, v in blocks:
+        request.digest += float((v * v).sum())
+
+
+class IntegralServer:
+    def __init__(self, budget_bytes=150e9, precision="mixed", max_inflight=3, slice_fraction=0.25,
+                 consumer=default_consumer, host_overlap=True, keep_blocks=False, fp32_threshold=None):
+        import torch
+
+        self.torch = torch
+        self.arena = Arena(torch, budget_bytes / 8)
+        self.precision = precision
+        self.fp32_threshold = fp32_threshold
+        self.max_inflight = max_inflight
+        self.slice_elems = int(self.arena.capacity * slice_fraction)
+        self.consumer = consumer
+        self.host_overlap = host_overlap
+        self.keep_blocks = keep_blocks
+        self.kept = collections.defaultdict(dict)
+        self.launches = 0
+
+    # -- request decomposition -------------------------------------------------
+    def _sliced(self, req, kind, pair_data):
+        mol = req.molecule
+        full = packed_elems(pair_data, req.aux_data)
+        if full <= self.slice_elems:
+            return [Piece(req, kind, pair_data, req.aux_data, 0, full)]
+        width = max(1, int(self.slice_elems / (full / mol.n_aux)))
+        return [Piece(req, kind, pair_data, sub, lo, packed_elems(pair_data, sub))
+                for lo, hi, sub in aux_slices(req.aux_data, mol.n_aux, width)]
+
+    def pieces_of(self, req):
+        mol = req.molecule
+        out = self._sliced(req, "3c", req.pair_data)
+        out += self._sliced(req, "metric", metric_pair_tables(req.aux_data))
+        charges = np.asarray(mol.geometry, np.float64).reshape(-1, 3)
+        out.append(Piece(req, "V", req.pair_data, {}, 0, packed_elems(req.pair_data, {}, len(charges)),
+                         charges=charges))
+        for p in out:
+            if p.elems > self.arena.capacity:
+                raise ValueError(f"request {req.rid}: one auxiliary shell slice exceeds the HBM budget")
+        return out
+
+    # -- S on a worker thread ----------------------------------------------------
+    def _host_worker(self, q):
+        from .molecular_integral import overlap
+
+        while True:
+            req = q.get()
+            if req is None:
+                return
+            req.S = overlap(req.pair_data, req.molecule)
+
+    # -- the loop ------------------------------------------------------------------
+    def serve(self, requests, realtime=True):
+        """Serve `requests` (each with .arrival seconds from start); returns stats.
+        realtime=False admits every request at once (arrival ignored)."""
+        todo = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        waiting = collections.deque()  # pieces of arrived requests, FIFO
+        inflight = []
+        hostq = queue.Queue()
+        worker = threading.Thread(target=self._host_worker, args=(hostq,), daemon=True)
+        if self.host_overlap:
+            worker.start()
+        t0 = time.perf_counter()
+        finished = []
+        n_total = len(todo)
+        try:
+            while len(finished) < n_total:
+                now = time.perf_counter() - t0
+                while todo and (todo[0].arrival <= now or not realtime):
+                    req = todo.popleft()
+                    if not realtime:
+                        req.arrival = now
+                    ps = self.pieces_of(req)
+                    req.pieces_left = len(ps)
+                    waiting.extend(ps)
+                    if self.host_overlap:
+                        hostq.put(req)
+                for item in list(inflight):
+                    if item[1].query():
+                        self._retire(item, finished, t0)
+                        inflight.remove(item)
+                if waiting and len(inflight) < self.max_inflight:
+                    largest = self.arena.largest_free
+                    group, total = [], 0
+                    while waiting and total + waiting[0].elems + 32 * (len(group) + 1) <= largest:
+                        p = waiting.popleft()
+                        group.append(p)
+                        total += p.elems
+                    if group:
+                        off, alloc = self.arena.alloc(total + 32 * len(group))
+                        inflight.append(self._launch(group, off, alloc))
+                        continue
+                    if not inflight:
+                        raise RuntimeError("a piece does not fit the empty arena")
+                if not inflight and not waiting and todo and realtime:
+                    time.sleep(max(0.0, min(0.002, todo[0].arrival - (time.perf_counter() - t0))))
+                else:
+                    time.sleep(0.0002)
+        finally:
+            for item in inflight:
+                item[0].sync()
+                item[0].close()
+            if self.host_overlap:
+                hostq.put(None)
+                worker.join()
+        wall = time.perf_counter() - t0
+        lat = np.array([r.done - r.arrival for r in finished])
+        return {"requests": n_total, "wall_s": wall, "throughput_rps": n_total / wall,
+                "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                "latency_mean_s": float(lat.mean()), "launches": self.launches}
+
+    def _launch(self, group, off, alloc):
+        """One batch (one CUDA-graph launch) over every piece of the group, its
+        output bound to the group's arena range; returns the in-flight record."""
+        torch = self.torch
+        kw = {} if self.fp32_threshold is None else {"fp32_threshold": self.fp32_threshold}
+        b = ThreeCenterBatch([p.request.molecule for p in group], [p.pair_data for p in group],
+                             [p.aux_data for p in group], precision=self.precision,
+                             charges_list=[p.charges for p in group], **kw)
+        if b.output_elems != sum(p.elems for p in group):
+            b.close()
+            raise RuntimeError("packed output size differs from the planned size")
+        b.bind_output(self.arena.buf.data_ptr() + 8 * off)
+        b.run(sync=False)
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.ExternalStream(b.stream))
+        self.launches += 1
+        return (b, ev, group, off, alloc)
+
+    def _retire(self, item, finished, t0):
+        batch, _, pieces, off, alloc = item
+        batch.status()
+        # the consumer's kernels run on torch's current stream: order them after the batch
+        torch = self.torch
+        torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(batch.stream))
+        for m, p in enumerate(pieces):
+            blocks = []
+            for li, lj, lk in p.classes():
+                blk = batch.block(m, li, lj, lk)
+                if blk is None:
+                    continue
+                o, nsp, nax = blk
+                n = nsp * (2 * li + 1) * (2 * lj + 1) * (2 * max(lk, 0) + 1) * nax
+                blocks.append(((li, lj, lk), self.arena.buf[off + o:off + o + n]))
+            self.consumer(p.request, p, blocks)
+            if self.keep_blocks:
+                for c, v in blocks:
+                    self.kept[p.request.rid][(p.kind, p.aux_lo) + c] = v.cpu().numpy().copy()
+            p.request.pieces_left -= 1
+            if p.request.pieces_left == 0:
+                p.request.done = time.perf_counter() - t0
+                finished.append(p.request)
+        # the consumer's work is queued on torch's stream; the range is reused
+        # only after it, so make the next batches wait for it
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream())
+        ev.synchronize()
+        self.arena.release(off, alloc)
+        batch.bind_output(0)
+        batch.close()

@@ -80,7 +80,7 @@ unsigned long long eip_kernel_launch_count(void);
 float eip_last_kernel_ms(void);
 
 /* Tuning variant (0..3) of the fast (mu nu|P) kernel of class (i_L, j_L | k_L),
- * i_L <= j_L <= 2, k_L <= 4: accumulator budget and register cap (see
+ * i_L <= j_L <= 2 or (i_L, j_L) = (0, 3), (0, 4), k_L <= 4: accumulator budget and register cap (see
  * k3c_fast.cuh).  Affects launches made after the call (a batch's graph keeps
  * the variants it was captured with).  set returns 1 for an invalid
  * class/variant; get returns -1 for a class without fast kernels. */
@@ -137,6 +137,13 @@ int eip_batch_add_pairs(eip_batch* batch, int molecule, int i_L, int j_L, const 
                         const int* pair_i_ao_start, const int* pair_j_ao_start, int n_pair);
 int eip_batch_add_aux(eip_batch* batch, int molecule, int k_L, const double* aux_A_a,
                       const double* aux_coefficient, const int* aux_i_aux_start, int n_primitive);
+/* Unit point charges at position[3 c .. 3 c + 2] (the charge_position argument
+ * of nuclear_attraction): adds the ket class k_L = EIP_POINT_CHARGES, whose
+ * blocks hold V[mu nu C] (not scaled by -Z), one "auxiliary shell" per charge
+ * with one component, always computed in FP64.  Charges of repeated calls for
+ * one molecule are numbered on in call order. */
+#define EIP_POINT_CHARGES (-1)
+int eip_batch_add_charges(eip_batch* batch, int molecule, const double* position, int n_charge);
 /* Precision of the batch (before build): mode 0 = FP64 everywhere (default);
  * mode 1 = mixed: a shell pair of a fast class is computed with FP32 R
  * tetrahedron, ket, bra and accumulation (FP64 Boys, R^m_000, E recurrences

@@ -128,3 +128,69 @@ def test_mixed_precision_within_1e10_of_fp64():
     assert err > 0.0  # the FP32 path really ran
     f64.close()
     mix.close()
+
+
+def _pq_close(a, b):
+    """(P|Q) reaches ~1e2: 1e-12 absolute where |v| <= 10, 1e-13 relative above."""
+    tol = np.maximum(1e-12, 1e-13 * np.abs(b))
+    err = np.abs(a - b)
+    assert np.all(err <= tol), float(np.max(err / tol))
+
+
+@pytest.mark.parametrize("omega", [0.0, 0.3])
+def test_batch_point_charges_match_nuclear_attraction(small_batch, omega):
+    """The point-charge ket class gives the drop-in nuclear_attraction V[mu nu C]
+    (and the reference library's) for every molecule of a batch."""
+    mols, pds, ads, _ = small_batch
+    charges = [m.geometry for m in mols]
+    b = bt.ThreeCenterBatch(mols, pds, ads, omega=omega, charges_list=charges)
+    b.alloc_output()
+    b.run()
+    b.status()
+    ref = oracle.reference()
+    for m in range(len(mols)):
+        V = b.dense_V(m)
+        np.testing.assert_allclose(V, mi.nuclear_attraction(pds[m], mols[m], charges[m], omega), rtol=0,
+                                   atol=1e-13)
+        if ref is not None:
+            np.testing.assert_allclose(V, oracle.drive_nuclear_attraction(ref, pds[m], mols[m], charges[m], omega),
+                                       rtol=0, atol=1e-12)
+    # the (mu nu|P) blocks are unchanged by the extra ket class
+    np.testing.assert_allclose(b.dense(2), mi.three_center(pds[2], ads[2], mols[2], omega), rtol=0, atol=1e-14)
+    b.close()
+
+
+@pytest.mark.parametrize("omega", [0.0, 0.3])
+def test_batch_metric_matches_two_center(small_batch, omega):
+    """(P|Q) as one-centre pair classes (0, l_P | l_Q) on the fast kernels equals
+    the drop-in two_center and the reference library."""
+    mols, _, ads, _ = small_batch
+    metric = [bt.metric_pair_tables(a) for a in ads]
+    b = bt.ThreeCenterBatch(mols, metric, ads, omega=omega)
+    b.alloc_output()
+    b.run()
+    b.status()
+    ref = oracle.reference()
+    for m in range(len(mols)):
+        M = b.dense_metric(m)
+        _pq_close(M, mi.two_center(ads[m], mols[m], omega))
+        if ref is not None:
+            _pq_close(M, oracle.drive_two_center(ref, ads[m], mols[m], omega))
+    b.close()
+
+
+def test_mixed_metric_within_1e10_of_fp64():
+    """The FP32 gate on one-centre (metric) pairs uses the auxiliary bound."""
+    m = _two_fragments()
+    ad = pu.form_auxiliary_pair_data(m)
+    metric = bt.metric_pair_tables(ad)
+    f64 = bt.ThreeCenterBatch([m], [metric], [ad], precision="fp64")
+    mix = bt.ThreeCenterBatch([m], [metric], [ad], precision="mixed")
+    for b in (f64, mix):
+        b.alloc_output()
+        b.run()
+        b.status()
+    err = np.max(np.abs(f64.dense_metric(0) - mix.dense_metric(0)))
+    assert err <= 1e-10, err
+    f64.close()
+    mix.close()
