@@ -21,6 +21,13 @@ buffer.  Metric unit: contracted shell triplets with Schwarz-type bound
   cpu_baseline  the reference library (oracle/_ref, its own C++/OpenMP path)
           on a bounded sample of the same molecules, all host cores.
 
+Also in the line (not part of the timed step): `dropin_fp64`, the plain FP64
+drop-in three_center on the cpu_baseline's sample; `serving`, a Poisson stream
+of 5-200-atom requests (S, V, (P|Q), (mu nu|P)) through the continuous-batching
+server, p50/p99 latency, beside the same requests served alone in FP64;
+`water100_mixed_vs_fp64`, the 100-water cluster's (mu nu|P) in FP64 and mixed
+precision window by window, max abs/rel error per class and triplets/s of both.
+
 `--impl reference` times only that reference path (per step: the sample) and
 prints its own line.  Under torchrun each rank runs its own 64 molecules
 (seed + rank): independent shards, no data-path collective (weak scaling).
@@ -225,7 +232,7 @@ def run_serving(args, torch, seed):
     return {
         "requests": n, "rate_rps": args.serve_rate, "atoms": [int(x) for x in sizes],
         "budget_gb": budget / 1e9, "precision": "mixed", "launches": st["launches"], "pieces": pieces,
-        "throughput_rps": st["throughput_rps"], "wall_s": st["wall_s"],
+        "throughput_rps": st["throughput_rps"], "wall_s": st["wall_s"], "host_s": st["host_s"],
         "latency_p50_ms": st["latency_p50_s"] * 1e3, "latency_p99_ms": st["latency_p99_s"] * 1e3,
         "alone_fp64": {"requests": len(alone), "sum_s": float(lat_alone.sum()),
                        "throughput_rps": len(alone) / float(lat_alone.sum()),
@@ -234,6 +241,93 @@ def run_serving(args, torch, seed):
                        "note": "each request served alone (nothing else in flight), FP64"
                                + ("" if frac == 1 else f", first {len(alone)} requests")},
         "sample": f"{n} of the 10k-request stream (Poisson {args.serve_rate} req/s, 5-200 atoms log-uniform)",
+    }
+
+
+def run_config2(torch, bt, threshold, seed=0, window_bytes=24e9):
+    """100-water cluster (300 atoms, 15 A cube, aux s-f): every (mu nu|P) in
+    FP64 and in mixed precision, window by window over the auxiliary basis on
+    resident tables; max abs / rel error of mixed vs FP64 per class, triplets/s
+    of both (screen 1e-12), and the FP64 (P|Q) metric."""
+    import importlib
+
+    syn = importlib.import_module("electron-integral-playground_b200.synthetic")
+    pu = importlib.import_module("electron-integral-playground_b200.pair_utility")
+    rf = importlib.import_module("electron-integral-playground_b200.roofline")
+    sv = importlib.import_module("electron-integral-playground_b200.serving")
+    mol = syn.config2_water100(seed)
+    pd, ad = pu.form_pair_data(mol, 1e-14), pu.form_auxiliary_pair_data(mol)
+    stats = rf.class_statistics(pd, ad, 1e-12)
+    screened = sum(v["screened"] for v in stats.values())
+    b64 = bt.ThreeCenterBatch([mol], [pd], [ad], precision="fp64")
+    bmx = bt.ThreeCenterBatch([mol], [pd], [ad], precision="mixed", fp32_threshold=threshold)
+    full = b64.window()
+    width = max(1, int(mol.n_aux * (window_bytes / 8) / full))
+    edges = sv.window_edges(ad, mol.n_aux, width)
+    sizes = [b64.window([lo], [hi]) for lo, hi in zip(edges[:-1], edges[1:])]
+    buf_a = torch.empty(max(sizes), dtype=torch.float64, device="cuda")
+    buf_b = torch.empty(max(sizes), dtype=torch.float64, device="cuda")
+    classes = [(li, lj, lk) for (li, lj) in pd for lk in ad]
+    err = {c: [0.0, 0.0] for c in classes}
+    ms = {"fp64": 0.0, "mixed": 0.0}
+    for lo, hi in zip(edges[:-1], edges[1:]):
+        for name, b, buf in (("fp64", b64, buf_a), ("mixed", bmx, buf_b)):
+            b.window([lo], [hi])
+            st = torch.cuda.ExternalStream(b.stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            b.run_window(buf.data_ptr())
+            e1.record(st)
+            b.sync()
+            ms[name] += e0.elapsed_time(e1)
+        for c in classes:
+            ba, bb = b64.window_block(0, *c), bmx.window_block(0, *c)
+            if ba is None or ba[2] == 0:
+                continue
+            n = ba[1] * (2 * c[0] + 1) * (2 * c[1] + 1) * (2 * c[2] + 1) * ba[2]
+            x, y = buf_a[ba[0]:ba[0] + n], buf_b[bb[0]:bb[0] + n]
+            d = (x - y).abs()
+            big = x.abs() > 1e-6
+            err[c][0] = max(err[c][0], float(d.max()))
+            if bool(big.any()):
+                err[c][1] = max(err[c][1], float((d[big] / x[big].abs()).max()))
+    b64.status()
+    bmx.status()
+    split = {c: bmx.precision_split(*c) for c in classes}
+    b64.close()
+    bmx.close()
+    del buf_a, buf_b
+    torch.cuda.empty_cache()
+    # (P|Q): FP64 (it feeds a Cholesky), one-centre pair classes on the same kernels
+    bm = bt.ThreeCenterBatch([mol], [bt.metric_pair_tables(ad)], [ad], precision="mixed")
+    bm.alloc_output()
+    bm.run()
+    st = torch.cuda.ExternalStream(bm.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    bm.run()
+    e1.record(st)
+    bm.sync()
+    bm.status()
+    pq_ms = e0.elapsed_time(e1)
+    pq_bytes = bm.output_bytes
+    bm.close()
+    torch.cuda.empty_cache()
+    n32 = sum(v[1] for v in split.values() if v)
+    n64 = sum(v[0] for v in split.values() if v)
+    return {
+        "workload": "100 waters in a 15 A cube (300 atoms), orbital O 3s2p1d / H 2s1p, aux s-f; "
+                    f"n_ao {mol.n_ao}, n_aux {mol.n_aux}",
+        "packed_output_bytes": 8 * full, "windows": len(sizes), "screened_triplets_1e-12": screened,
+        "fp64": {"ms": ms["fp64"], "triplets_per_s": screened / (ms["fp64"] * 1e-3)},
+        "mixed": {"ms": ms["mixed"], "triplets_per_s": screened / (ms["mixed"] * 1e-3),
+                  "fp32_threshold": threshold, "fp32_fraction_of_triplets": n32 / max(1, n32 + n64)},
+        "mixed_vs_fp64_by_class": {f"{c[0]}{c[1]}|{c[2]}": {"max_abs": e[0], "max_rel_where_abs_gt_1e-6": e[1],
+                                                             "fp32_triplets": split[c][1] if split[c] else 0}
+                                   for c, e in sorted(err.items())},
+        "max_abs_all_classes": max(e[0] for e in err.values()),
+        "metric_PQ": {"precision": "fp64 (one-centre pairs never take the FP32 path)", "ms": pq_ms,
+                      "bytes": pq_bytes},
     }
 
 
@@ -279,6 +373,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=24, help="serving sample: requests (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="serving sample: Poisson arrival rate, req/s")
     ap.add_argument("--serve-alone", type=int, default=24, help="requests also timed alone in FP64")
+    ap.add_argument("--no-config2", action="store_true",
+                    help="skip the 100-water mixed-vs-FP64 per-class measurement")
     ap.add_argument("--tune", action="store_true",
                     help="run the autotuner on this workload first and rewrite its cache")
     args = ap.parse_args()
@@ -440,6 +536,7 @@ def main():
                              f"{smp['triplets']} screened triplets, {smp['seconds']:.1f} s"}
             dropin = dropin_sample(mols, pds, ads, stats, smp["molecules"])
     serving = run_serving(args, torch, args.seed + 1000 * rank) if args.serve_requests > 0 else None
+    config2 = run_config2(torch, bt, args.fp32_threshold, args.seed) if not args.no_config2 and rank == 0 else None
     if rank == 0:
         per = head["per_step"]
         line = {
@@ -469,6 +566,7 @@ def main():
                     "fp64_value": screened / (m64["e2e_ms"] * 1e-3),
                     "result": "per-molecule checksum of the packed (mu nu|P) (computed in the kernels' epilogue)"},
             "roofline": roof, "cpu_baseline": cpu, "dropin_fp64": dropin, "serving": serving,
+            "water100_mixed_vs_fp64": config2,
             "gpu_launches": head["launches"], "clocks": head["clocks"], "clocks_fp64": m64["clocks"],
             "latency_ms": {"p50": statistics.median(per), "p99": sorted(per)[min(len(per) - 1, int(0.99 * len(per)))],
                            "what": "per-step (whole batch) device time; request latency is under serving"},

@@ -15,7 +15,7 @@ import pathlib
 
 from ._lib import lib
 
-N_VARIANTS = 4
+N_VARIANTS = 6
 DEFAULT_CACHE = pathlib.Path(__file__).resolve().parent / "tuning" / "b200_fp64.json"
 
 

@@ -72,6 +72,10 @@ def _bind(L):
     L.eip_batch_output_device.restype = _vp
     L.eip_batch_run.argtypes = [_vp, c_int]
     L.eip_batch_run_class.argtypes = [_vp, c_int, c_int, c_int]
+    L.eip_batch_window_plan.argtypes = [_vp, _ipp, _ipp, c_int]
+    L.eip_batch_window_plan.restype = c_ll
+    L.eip_batch_window_block.argtypes = [_vp, c_int, c_int, c_int, c_int, ctypes.POINTER(c_ll), _ipp, _ipp]
+    L.eip_batch_run_window.argtypes = [_vp, _vp, c_int]
     L.eip_batch_sync.argtypes = [_vp]
     L.eip_batch_status.argtypes = [_vp]
     L.eip_batch_upload.argtypes = [_vp]
@@ -175,6 +179,34 @@ class ThreeCenterBatch:
             return False
         self._check(rc, "run_class")
         return True
+
+    def window(self, fn_lo=None, fn_hi=None, with_charges=False):
+        """Select the auxiliary window [fn_lo[m], fn_hi[m]) of every molecule
+        (None: all functions); returns the window's packed output size."""
+        if (fn_lo is None) != (fn_hi is None):
+            raise ValueError("give both window bounds or neither")
+        if fn_lo is not None:
+            lo = as_i32(np.broadcast_to(np.asarray(fn_lo), (len(self.molecules),)))
+            hi = as_i32(np.broadcast_to(np.asarray(fn_hi), (len(self.molecules),)))
+            n = self.L.eip_batch_window_plan(self.h, ip(lo), ip(hi), 1 if with_charges else 0)
+        else:
+            n = self.L.eip_batch_window_plan(self.h, None, None, 1 if with_charges else 0)
+        if n < 0:
+            raise IntegralError(f"eip_batch_window_plan: {self.L.eip_batch_error(self.h).decode(errors='replace')}")
+        return int(n)
+
+    def window_block(self, m, li, lj, lk):
+        off, nsp, nax = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int()
+        rc = self.L.eip_batch_window_block(self.h, m, li, lj, lk, ctypes.byref(off), ctypes.byref(nsp),
+                                           ctypes.byref(nax))
+        if rc != 0:
+            return None
+        return off.value, nsp.value, nax.value
+
+    def run_window(self, device_ptr: int, checksum: bool = False):
+        """Launch the selected window into device memory at device_ptr (async)."""
+        self._check(self.L.eip_batch_run_window(self.h, ctypes.c_void_p(device_ptr), 1 if checksum else 0),
+                    "run_window")
 
     def sync(self):
         self._check(self.L.eip_batch_sync(self.h), "sync")

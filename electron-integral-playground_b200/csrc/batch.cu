@@ -58,6 +58,12 @@ struct ClassPlan {
     int* counter32 = nullptr;
     long long triplets32 = 0, triplets64 = 0;
     int n_sp_total32 = 0;
+    std::vector<int> n64, n32;          // per molecule: shell pairs on the FP64 / FP32 list
+    // auxiliary window (eip_batch_window_plan): per molecule output offset and shells
+    size_t win_off = 0;                 // this plan's arrays in the window buffers
+    int win_items64 = 0, win_items32 = 0;
+    std::vector<long long> win_out;
+    std::vector<int> win_start, win_count;
     std::vector<long long> out_begin;   // per molecule
     std::vector<int> n_sp, n_auxsh;     // per molecule
     std::vector<int> sp0, aux0;         // per molecule (global indices in class tables)
@@ -111,6 +117,21 @@ struct eip_batch {
     std::map<std::pair<int, int>, size_t> etab_offset;
     std::map<std::pair<int, int>, std::vector<int>> bra_sp_begin;  // per molecule prefix
     std::map<int, std::vector<int>> ket_aux_begin;
+    std::map<int, std::vector<int>> ket_start;  // per class: first function of every auxiliary shell
+    // auxiliary-window runs: per-plan maps in a ring of kWinSlots pinned buffers
+    // mirrored on the device, so a window can be planned while earlier ones run
+    static constexpr int kWinSlots = 4;
+    void* h_win = nullptr;
+    void* d_win = nullptr;
+    size_t win_bytes = 0;  // one slot
+    int win_slot = 0;      // slot of the planned window
+    int win_next = 0;
+    cudaEvent_t win_uploaded[kWinSlots] = {};  // the slot's last upload has been read
+    bool win_pending[kWinSlots] = {};
+    bool win_planned = false;
+    bool win_charges = false;
+    long long win_elems = 0;
+    bool etab_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     unsigned long long launches_per_run = 0;
@@ -153,13 +174,12 @@ void group_indices(const int* ia, const int* ja, int n, std::vector<int>& order,
 // distance shift applied once: 2 |c_a c_b| (la/2ea)^(la/2) (lb/2eb)^(lb/2)
 // exp(-ab/p d^2) max((pi/p)^1.5, 2^0.25 (pi/p)^1.25), d = max(|AB| - sqrt(la/2a)
 // - sqrt(lb/2b), 0); |c_a c_b| recovered from c_ab = c_a c_b exp(-ab/p |AB|^2).
-double aux_bound(double q, double coef, int l);
-
 double pair_bound(const double* A, const double* B, double coef, int la, int lb) {
     // A one-centre "pair" (an s function of exponent 0 times one Gaussian: the
-    // bra of the two-centre metric run as a three-centre class) is bounded
-    // like an auxiliary function.
-    if (A[3] == 0.0 && la == 0) return aux_bound(B[3], coef, lb);
+    // bra of the two-centre metric (P|Q) run as a three-centre class) gets an
+    // infinite bound: the metric, which feeds a Cholesky factorisation, stays
+    // FP64 in mixed mode.
+    if (A[3] == 0.0 && la == 0) return HUGE_VAL;
     const double a = A[3], b = B[3], p = a + b, mu = a * b / p;
     const double dx = A[0] - B[0], dy = A[1] - B[1], dz = A[2] - B[2];
     const double ab2 = dx * dx + dy * dy + dz * dz, ab = sqrt(ab2);
@@ -432,6 +452,8 @@ int eip_batch_build(eip_batch* b) {
             }
             pl.triplets32 += (long long)n32 * pl.n_auxsh[m];
             pl.triplets64 += (long long)n64 * pl.n_auxsh[m];
+            pl.n64.push_back(n64);
+            pl.n32.push_back(n32);
             ib64[m + 1] = ib64[m] + n64 * tiles;
             ib32[m + 1] = ib32[m] + n32 * tiles;
             lb64[m + 1] = lb64[m] + n64;
@@ -496,6 +518,7 @@ int eip_batch_build(eip_batch* b) {
         ket_by_class[kv.first] =
             KetTable{(int)H.start.size(), at<int>(d, o.beg), at<int>(d, o.st), at<double4>(d, o.c), at<double>(d, o.co)};
         b->ket_aux_begin[kv.first] = H.aux_begin;
+        b->ket_start[kv.first] = H.start;
     }
     for (size_t i = 0; i < b->plans.size(); i++) {
         ClassPlan& pl = b->plans[i];
@@ -520,6 +543,20 @@ int eip_batch_build(eip_batch* b) {
             // all pairs in FP64: plain numbering, sp_begin = the molecule's first pair
             pl.map = BatchMap{nm, dp, dp + 5 * (nm + 1), dp + 2 * (nm + 1), dob, nullptr, nullptr, nullptr};
         }
+    }
+    // window maps: per plan [item_begin64 | item_begin32 (n_mol + 1 each) | aux start |
+    // aux count (n_mol each)], then the 8-byte aligned out_begin (n_mol)
+    {
+        Layout W;
+        for (ClassPlan& pl : b->plans) pl.win_off = W.add(sizeof(int) * (4 * nm + 2) + 8 + sizeof(long long) * nm);
+        b->win_bytes = std::max<size_t>(W.total, 256);
+        if ((e = cudaMallocHost(&b->h_win, b->win_bytes * eip_batch::kWinSlots)) != cudaSuccess)
+            return fail(b, "pinned window maps", e);
+        if ((e = cudaMalloc(&b->d_win, b->win_bytes * eip_batch::kWinSlots)) != cudaSuccess)
+            return fail(b, "window maps", e);
+        for (int i = 0; i < eip_batch::kWinSlots; i++)
+            if ((e = cudaEventCreateWithFlags(&b->win_uploaded[i], cudaEventDisableTiming)) != cudaSuccess)
+                return fail(b, "event", e);
     }
     if ((e = cudaMemcpyAsync(d, h, L.total, cudaMemcpyHostToDevice, b->stream)) != cudaSuccess)
         return fail(b, "table upload", e);
@@ -605,7 +642,8 @@ static int capture(eip_batch* b, bool checksum) {
     int next = 0;
     for (ClassPlan& pl : b->plans) {
         if (pl.total_items == 0 && pl.total_items32 == 0) continue;
-        cudaStream_t s = b->side[next++ % n_side];
+        // generic classes share d_scratch: all of them go to the first side stream
+        cudaStream_t s = pl.fast ? b->side[next++ % n_side] : b->side[0];
         if (pl.fast) {
             if (pl.total_items > 0) {
                 BatchMap map = pl.map;
@@ -684,6 +722,186 @@ int eip_batch_run_class(eip_batch* b, int i_L, int j_L, int k_L) {
     return 1;
 }
 
+static size_t win_ob_off(int nm) { return ((sizeof(int) * (4 * nm + 2)) + 7) & ~size_t(7); }
+
+long long eip_batch_window_plan(eip_batch* b, const int* fn_lo, const int* fn_hi, int with_charges) {
+    if (!b || !b->built) return -1;
+    const int nm = b->n_mol;
+    // next slot of the ring; its pinned maps may still be in an earlier upload
+    const int slot = b->win_next;
+    if (b->win_pending[slot]) {
+        cudaError_t e = cudaEventSynchronize(b->win_uploaded[slot]);
+        if (e != cudaSuccess) {
+            fail(b, "window upload", e);
+            return -1;
+        }
+        b->win_pending[slot] = false;
+    }
+    void* hw = static_cast<char*>(b->h_win) + b->win_bytes * slot;
+    long long total = 0;
+    for (ClassPlan& pl : b->plans) {
+        int* v = at<int>(hw, pl.win_off);
+        int* ib64 = v;
+        int* ib32 = v + (nm + 1);
+        int* ast = v + 2 * (nm + 1);
+        int* acnt = ast + nm;
+        long long* ob = at<long long>(hw, pl.win_off + win_ob_off(nm));
+        const std::vector<int>& starts = b->ket_start[pl.lk];
+        const std::vector<int>& ab = b->ket_aux_begin[pl.lk];
+        const int lk = pl.point ? 0 : pl.lk;
+        const long long blk_unit = (long long)(b->spherical ? nsph(pl.li) * nsph(pl.lj) * nsph(lk)
+                                                            : ncart(pl.li) * ncart(pl.lj) * ncart(lk));
+        pl.win_out.assign(nm, 0);
+        pl.win_start.assign(nm, 0);
+        pl.win_count.assign(nm, 0);
+        ib64[0] = ib32[0] = 0;
+        for (int m = 0; m < nm; m++) {
+            int s0 = ab[m], s1 = ab[m];
+            if (!pl.point || with_charges) {
+                s0 = ab[m];
+                s1 = ab[m + 1];
+                if (!pl.point && fn_lo && fn_hi) {
+                    s0 = (int)(std::lower_bound(starts.begin() + ab[m], starts.begin() + ab[m + 1], fn_lo[m]) -
+                               starts.begin());
+                    s1 = (int)(std::lower_bound(starts.begin() + s0, starts.begin() + ab[m + 1], fn_hi[m]) -
+                               starts.begin());
+                }
+            }
+            const int cnt = s1 - s0, tiles = (cnt + 31) / 32;
+            ast[m] = s0;
+            acnt[m] = cnt;
+            ob[m] = total;
+            pl.win_out[m] = total;
+            pl.win_start[m] = s0;
+            pl.win_count[m] = cnt;
+            total += (long long)pl.n_sp[m] * cnt * blk_unit;
+            const long long i64 = (long long)ib64[m] + (long long)pl.n64[m] * tiles;
+            const long long i32 = (long long)ib32[m] + (long long)pl.n32[m] * tiles;
+            if (i64 > 0x7fffffffLL || i32 > 0x7fffffffLL) {
+                fail(b, "window too large", cudaSuccess);
+                return -1;
+            }
+            ib64[m + 1] = (int)i64;
+            ib32[m + 1] = (int)i32;
+        }
+        pl.win_items64 = ib64[nm];
+        pl.win_items32 = ib32[nm];
+    }
+    b->win_elems = total;
+    b->win_slot = slot;
+    b->win_next = (slot + 1) % eip_batch::kWinSlots;
+    b->win_planned = true;
+    b->win_charges = with_charges != 0;
+    return total;
+}
+
+int eip_batch_window_block(eip_batch* b, int mol, int i_L, int j_L, int k_L, long long* offset, int* n_pair_shells,
+                           int* n_aux_shells) {
+    if (!b || !b->built || !b->win_planned || mol < 0 || mol >= b->n_mol) return 2;
+    for (const ClassPlan& pl : b->plans)
+        if (pl.li == i_L && pl.lj == j_L && pl.lk == k_L) {
+            *offset = pl.win_out[mol];
+            *n_pair_shells = pl.n_sp[mol];
+            *n_aux_shells = pl.win_count[mol];
+            return 0;
+        }
+    return 1;
+}
+
+int eip_batch_run_window(eip_batch* b, double* device_out, int checksum) {
+    if (!b || !b->built || !b->win_planned || !device_out) return 2;
+    cudaError_t e;
+    const int nm = b->n_mol;
+    const int n_side = 4;
+    if (b->side.empty()) {
+        for (int i = 0; i < n_side; i++) {
+            cudaStream_t s;
+            if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess) return fail(b, "stream", e);
+            b->side.push_back(s);
+        }
+        for (int i = 0; i < 2 * n_side + 1; i++) {
+            cudaEvent_t ev;
+            if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(b, "event", e);
+            b->events.push_back(ev);
+        }
+    }
+    const int slot = b->win_slot;
+    void* dw = static_cast<char*>(b->d_win) + b->win_bytes * slot;
+    if ((e = cudaMemcpyAsync(dw, static_cast<char*>(b->h_win) + b->win_bytes * slot, b->win_bytes,
+                             cudaMemcpyHostToDevice, b->stream)) != cudaSuccess)
+        return fail(b, "window upload", e);
+    cudaEventRecord(b->win_uploaded[slot], b->stream);
+    b->win_pending[slot] = true;
+    int rc = 0;
+    if (!b->etab_ready) {
+        for (auto& kv : b->bra_by_class) {
+            if (!fast3c_supported(kv.first.first, kv.first.second, 0) || !b->spherical) continue;
+            rc |= launch_e_table(kv.first.first, kv.first.second, kv.second, b->d_etab + b->etab_offset[kv.first],
+                                 b->stream);
+        }
+        b->etab_ready = true;
+    }
+    if (checksum) cudaMemsetAsync(b->d_checksum, 0, sizeof(double) * nm, b->stream);
+    cudaEventRecord(b->events[0], b->stream);
+    for (int i = 0; i < n_side; i++) cudaStreamWaitEvent(b->side[i], b->events[0], 0);
+    int next = 0;
+    for (ClassPlan& pl : b->plans) {
+        if (pl.win_items64 == 0 && pl.win_items32 == 0) continue;
+        cudaStream_t s = pl.fast ? b->side[next++ % n_side] : b->side[0];  // generic: shared scratch
+        const int* v = at<int>(dw, pl.win_off);
+        const int* ast = v + 2 * (nm + 1);
+        const long long* ob = at<long long>(dw, pl.win_off + win_ob_off(nm));
+        if (pl.fast) {
+            cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), s);
+            if (pl.win_items64 > 0) {
+                BatchMap map = pl.map;
+                map.item_begin = v;
+                map.aux_begin = ast;
+                map.aux_count = ast + nm;
+                map.out_begin = ob;
+                map.checksum = checksum ? b->d_checksum : nullptr;
+                rc |= pl.point ? launch_fast_point(pl.li, pl.lj, pl.bra, pl.ket, map, pl.win_items64, b->omega,
+                                                   device_out, pl.counter, s)
+                               : launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, map, pl.win_items64, b->omega,
+                                               device_out, pl.counter, s);
+            }
+            if (pl.win_items32 > 0) {
+                BatchMap map = pl.map32;
+                map.item_begin = v + (nm + 1);
+                map.aux_begin = ast;
+                map.aux_count = ast + nm;
+                map.out_begin = ob;
+                map.checksum = checksum ? b->d_checksum : nullptr;
+                rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, map, pl.win_items32, b->omega, device_out,
+                                    pl.counter32, s, true);
+            }
+        } else {
+            const int lk = pl.point ? 0 : pl.lk;
+            for (int m = 0; m < nm; m++) {
+                if (pl.n_sp[m] == 0 || pl.win_count[m] == 0) continue;
+                BraTable bra = pl.bra;
+                bra.n_group = pl.n_sp[m];
+                bra.grp_begin += pl.sp0[m];
+                bra.grp_ao += pl.sp0[m];
+                bra.grp_AB += pl.sp0[m];
+                KetTable ket = pl.ket;
+                ket.n_group = pl.win_count[m];
+                ket.grp_begin += pl.win_start[m];
+                ket.grp_start += pl.win_start[m];
+                rc |= launch_generic_raw(pl.point ? 1 : 0, pl.li, pl.lj, lk, bra, ket, b->omega, 0, b->d_scratch, s);
+                rc |= launch_transform(pl.li, pl.lj, lk, b->spherical, pl.n_sp[m], pl.win_count[m], b->d_scratch,
+                                       device_out + pl.win_out[m], s);
+            }
+        }
+    }
+    for (int i = 0; i < n_side; i++) {
+        cudaEventRecord(b->events[1 + i], b->side[i]);
+        cudaStreamWaitEvent(b->stream, b->events[1 + i], 0);
+    }
+    if (rc != 0) return fail(b, "window launch", cudaGetLastError());
+    return 0;
+}
+
 int eip_batch_precision_split(eip_batch* b, int i_L, int j_L, int k_L, long long* triplets_fp64,
                               long long* triplets_fp32) {
     if (!b || !b->built) return 2;
@@ -758,6 +976,10 @@ void eip_batch_destroy(eip_batch* b) {
     if (b->d_etab) cudaFree(b->d_etab);
     if (b->d_checksum) cudaFree(b->d_checksum);
     if (b->d_scratch) cudaFree(b->d_scratch);
+    if (b->d_win) cudaFree(b->d_win);
+    if (b->h_win) cudaFreeHost(b->h_win);
+    for (auto ev : b->win_uploaded)
+        if (ev) cudaEventDestroy(ev);
     for (auto s : b->side) cudaStreamDestroy(s);
     for (auto ev : b->events) cudaEventDestroy(ev);
     if (b->stream) cudaStreamDestroy(b->stream);

@@ -234,15 +234,20 @@ struct BraTable {
 // class each take a subset of the shell pairs): when sp_list is set, molecule
 // m's k-th pair is sp_list[sp_begin[m] + k] (a global index) and its output
 // row is that index minus sp_first[m], the molecule's first pair.
+//
+// Optional auxiliary window: when aux_count is set, molecule m's auxiliary
+// shells are [aux_begin[m], aux_begin[m] + aux_count[m]) (a run over a window
+// of each molecule's auxiliary basis) instead of up to aux_begin[m + 1].
 struct BatchMap {
     int n_mol;
     const int* item_begin;  // n_mol + 1
     const int* sp_begin;    // n_mol + 1
-    const int* aux_begin;   // n_mol + 1
+    const int* aux_begin;   // n_mol + 1 (n_mol with aux_count)
     const long long* out_begin;
     double* checksum;
     const int* sp_list;   // optional
     const int* sp_first;  // n_mol, with sp_list
+    const int* aux_count = nullptr;  // optional, n_mol
 };
 
 // One-centre ("ket") table: auxiliary shells of one class (or point charges).

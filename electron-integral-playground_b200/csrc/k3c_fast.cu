@@ -11,7 +11,8 @@ namespace eip {
                                     const BatchMap& map, int total_items, double omega, double* out,         \
                                     int* counter, cudaStream_t s);
 #define EIP_DECL(I, J)                                                                                      \
-    EIP_DECL_V(I, J, 0) EIP_DECL_V(I, J, 1) EIP_DECL_V(I, J, 2) EIP_DECL_V(I, J, 3)                         \
+    EIP_DECL_V(I, J, 0) EIP_DECL_V(I, J, 1) EIP_DECL_V(I, J, 2) EIP_DECL_V(I, J, 3) EIP_DECL_V(I, J, 4)     \
+    EIP_DECL_V(I, J, 5)                                                                                     \
     int launch_fast3c_##I##J##_f32(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket, \
                                    const BatchMap& map, int total_items, double omega, double* out,         \
                                    int* counter, cudaStream_t s);                                           \
@@ -36,7 +37,7 @@ int fast3c_variant(int li, int lj, int lk) {
 }
 
 int fast3c_set_variant(int li, int lj, int lk, int v) {
-    if (!fast3c_supported(li, lj, lk) || v < 0 || v > 3) return 1;
+    if (!fast3c_supported(li, lj, lk) || v < 0 || v > 5) return 1;
     g_variant[li][lj][lk] = v;
     return 0;
 }
@@ -52,14 +53,16 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
                   int total_items, double omega, double* out, int* counter, cudaStream_t s, bool fp32) {
     if (!fast3c_supported(li, lj, lk)) return 1;
     const double* t = boys_table_device();
-    const int v = fp32 ? 4 : g_variant[li][lj][lk];
+    const int v = fp32 ? -1 : g_variant[li][lj][lk];
 #define EIP_GO_V(I, J, V) return launch_fast3c_##I##J##_v##V(lk, t, bra, ket, map, total_items, omega, out, counter, s)
 #define EIP_GO(I, J)                                                                                          \
     switch (v) {                                                                                              \
         case 1: EIP_GO_V(I, J, 1);                                                                            \
         case 2: EIP_GO_V(I, J, 2);                                                                            \
         case 3: EIP_GO_V(I, J, 3);                                                                            \
-        case 4: return launch_fast3c_##I##J##_f32(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
+        case 4: EIP_GO_V(I, J, 4);                                                                            \
+        case 5: EIP_GO_V(I, J, 5);                                                                            \
+        case -1: return launch_fast3c_##I##J##_f32(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
         default: EIP_GO_V(I, J, 0);                                                                           \
     }
     switch (li * 10 + lj) {

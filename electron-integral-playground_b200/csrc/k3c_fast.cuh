@@ -36,9 +36,10 @@ namespace eip {
 //   ACC   accumulators (doubles) per lane -> how many warps split the ket
 //   WARPS resident warps per SM asked of the register allocator (register cap
 //         65536 / (32 * WARPS)); more warps hide latency, fewer avoid spills.
-constexpr int kVariants = 4;
-__host__ __device__ constexpr int variant_acc(int v) { return v == 2 ? 24 : (v == 3 ? 96 : 48); }
-__host__ __device__ constexpr int variant_warps(int v) { return v == 1 || v == 3 ? 8 : 16; }
+//   v0 48/16, v1 48/8, v2 24/16, v3 96/8, v4 24/24, v5 48/24
+constexpr int kVariants = 6;
+__host__ __device__ constexpr int variant_acc(int v) { return v == 2 || v == 4 ? 24 : (v == 3 ? 96 : 48); }
+__host__ __device__ constexpr int variant_warps(int v) { return v == 1 || v == 3 ? 8 : (v >= 4 ? 24 : 16); }
 
 template <int LI, int LJ, int LK, int V = 0>
 struct Fast3c {
@@ -57,6 +58,13 @@ struct Fast3c {
     static constexpr int THREADS = 32 * KS;
     // resident CTAs per SM asked of the register allocator
     static constexpr int MIN_CTAS = (variant_warps(V) / KS) < 1 ? 1 : (variant_warps(V) / KS);
+    // units (primitive pair x auxiliary primitive) per block, doubles per unit and lane
+    static constexpr int UB = KS;
+    static constexpr int NU = L + 6;
+    template <typename T>
+    static constexpr size_t smem_bytes() {
+        return sizeof(double) * UB * NU * 32 + sizeof(T) * (NR * 32 + UB * 3 * NE);
+    }
 };
 
 // Ket coefficient table of one l_k: for spherical component ko and Hermite
@@ -158,8 +166,15 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
          double* __restrict__ out, int* __restrict__ work_counter, int total_items) {
     using C = Fast3c<LI, LJ, LK, V>;
     constexpr int L = C::L;
-    __shared__ T sE[3 * C::NE];
-    __shared__ T sR[C::NR * 32];
+    constexpr int UB = C::UB;
+    constexpr int NU = C::NU;
+    // dynamic shared memory (fast3c_smem_bytes): per block of UB units
+    // (primitive pair x auxiliary primitive) the lanes' R^(m)_000 and unit
+    // data, then the R tetrahedron of the current unit, then the units' E tables
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sU = reinterpret_cast<double*>(smem_raw);  // [UB][NU][32]
+    T* sR = reinterpret_cast<T*>(sU + UB * NU * 32);    // [NR][32]
+    T* sE = sR + C::NR * 32;                            // [UB][3 NE]
     __shared__ int s_item;
 
     const int lane = threadIdx.x & 31;
@@ -189,7 +204,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
         }
         const int m = lo;
         const int aux0 = __ldg(map.aux_begin + m);
-        const int n_aux = __ldg(map.aux_begin + m + 1) - aux0;
+        const int n_aux = map.aux_count ? __ldg(map.aux_count + m) : __ldg(map.aux_begin + m + 1) - aux0;
         const int n_tiles = (n_aux + 31) >> 5;
         const int local = item - __ldg(map.item_begin + m);
         const int sp_k = local / n_tiles;
@@ -225,13 +240,25 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
 #pragma unroll
             for (int c = 0; c < C::KPW; c++) acc[i][c] = T(0);
 
-        for (int pp = pb; pp < pe; pp++) {
-            const double4 P = bra.prim_P[pp];
-            const double4 PA = bra.prim_PA[pp];
-            const double p = P.w;
-            for (int e = threadIdx.x; e < 3 * C::NE; e += C::THREADS)
-                sE[e] = (T)__ldg(bra.prim_E + (size_t)pp * 3 * C::NE + e);
-            for (int kk = 0; kk < nk_max; kk++) {
+        // Units u = (primitive pair, auxiliary primitive) in blocks of UB: the
+        // warps first evaluate the units' Boys functions and prefactors in
+        // parallel (one warp per unit, no redundancy), then go through the
+        // units one by one, splitting each unit's R tetrahedron and ket
+        // components between them.
+        const int n_units = (pe - pb) * nk_max;
+        for (int u0 = 0; u0 < n_units; u0 += UB) {
+            const int nb = n_units - u0 < UB ? n_units - u0 : UB;
+            for (int e = threadIdx.x; e < nb * 3 * C::NE; e += C::THREADS) {
+                const int ub = e / (3 * C::NE), r = e - ub * (3 * C::NE);
+                const int pp = pb + (u0 + ub) / nk_max;
+                sE[e] = (T)__ldg(bra.prim_E + (size_t)pp * 3 * C::NE + r);
+            }
+            for (int ub = warp; ub < nb; ub += C::KS) {
+                const int u = u0 + ub;
+                const int pp = pb + u / nk_max, kk = u - (u / nk_max) * nk_max;
+                const double4 P = bra.prim_P[pp];
+                const double4 PA = bra.prim_PA[pp];
+                const double p = P.w;
                 const bool live = kk < nk;
                 const double4 Cq = live ? ket.prim_C[kb + kk] : make_double4(P.x, P.y, P.z, 1.0);
                 const double cc = live ? ket.prim_coef[kb + kk] : 0.0;
@@ -255,25 +282,36 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                     pref64 = PA.w * cc * kTwoPi52 * omega / (p * q * sqrt(p * q + (p + q) * omega * omega));
                 }
                 if (LK & 1) pref64 = -pref64;  // (-1)^{|s|} with |s| = LK mod 2
-                const T pref = (T)pref64;
-
-                // R^{(m)}_000 = (-2 zeta)^m F_m(zeta |PQ|^2); this warp's share of
-                // the tetrahedron by the closed form (entries are independent).
+                // R^{(m)}_000 = (-2 zeta)^m F_m(zeta |PQ|^2)
                 double Rm[L + 1];
                 boys<L>(boys_table, zeta * (X * X + Y * Y + Z * Z), Rm);
-                {
-                    const double f = -2.0 * zeta;
-                    double g = f;
+                double* unit = sU + ub * NU * 32 + lane;
+                const double f = -2.0 * zeta;
+                double g = 1.0;
 #pragma unroll
-                    for (int mm = 1; mm <= L; mm++) {
-                        Rm[mm] *= g;
-                        g *= f;
-                    }
+                for (int mm = 0; mm <= L; mm++) {
+                    unit[mm * 32] = Rm[mm] * g;
+                    g *= f;
                 }
+                unit[(L + 1) * 32] = X;
+                unit[(L + 2) * 32] = Y;
+                unit[(L + 3) * 32] = Z;
+                unit[(L + 4) * 32] = pref64;
+                unit[(L + 5) * 32] = q;
+            }
+            __syncthreads();
+            for (int ub = 0; ub < nb; ub++) {
+                const double* unit = sU + ub * NU * 32 + lane;
+                const T* sEu = sE + ub * (3 * C::NE);
+                const double X = unit[(L + 1) * 32], Y = unit[(L + 2) * 32], Z = unit[(L + 3) * 32];
+                const T pref = (T)unit[(L + 4) * 32];
+                const double q = unit[(L + 5) * 32];
+                // this warp's share of the tetrahedron by the closed form
+                // (entries are independent)
                 T Rt[L + 1], px[L + 1], py[L + 1], pz[L + 1];
                 px[0] = py[0] = pz[0] = T(1);
 #pragma unroll
-                for (int mm = 0; mm <= L; mm++) Rt[mm] = (T)Rm[mm];
+                for (int mm = 0; mm <= L; mm++) Rt[mm] = (T)unit[mm * 32];
 #pragma unroll
                 for (int mm = 1; mm <= L; mm++) {
                     px[mm] = px[mm - 1] * (T)X;
@@ -419,15 +457,15 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                                 for (int c = 0; c < C::KPW; c++) sv[c] = T(0);
                                 static_for<0, iz + jz + 1>([&](auto v_) {
                                     constexpr int v = decltype(v_)::value;
-                                    const T ez = sE[2 * C::NE + e_offset<LJ>(iz, jz) + v];
+                                    const T ez = sEu[2 * C::NE + e_offset<LJ>(iz, jz) + v];
 #pragma unroll
                                     for (int c = 0; c < C::KPW; c++) sv[c] = fma(ez, Xh[c][herm_index(t, u, v)], sv[c]);
                                 });
-                                const T ey = sE[C::NE + e_offset<LJ>(iy, jy) + u];
+                                const T ey = sEu[C::NE + e_offset<LJ>(iy, jy) + u];
 #pragma unroll
                                 for (int c = 0; c < C::KPW; c++) su[c] = fma(ey, sv[c], su[c]);
                             });
-                            const T ex = sE[e_offset<LJ>(ix, jx) + t];
+                            const T ex = sEu[e_offset<LJ>(ix, jx) + t];
 #pragma unroll
                             for (int c = 0; c < C::KPW; c++) sxv[c] = fma(ex, su[c], sxv[c]);
                         });
@@ -488,19 +526,23 @@ static int launch_one(const double* boys_table, const BraTable& bra, const KetTa
                       int total_items, double omega, double* out, int* counter, cudaStream_t s) {
     using C = Fast3c<LI, LJ, LK, V>;
     if (total_items <= 0) return 0;
+    constexpr size_t smem = C::template smem_bytes<T>();
     static int max_blocks = 0;
     if (max_blocks == 0) {
         int per_sm = 0, dev = 0, sms = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3c_fast<LI, LJ, LK, V, T, POINT>, C::THREADS, 0) !=
-            cudaSuccess)
+        if (cudaFuncSetAttribute(k3c_fast<LI, LJ, LK, V, T, POINT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return 2;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3c_fast<LI, LJ, LK, V, T, POINT>, C::THREADS,
+                                                          smem) != cudaSuccess)
             return 2;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         max_blocks = (per_sm < 1 ? 1 : per_sm) * sms;
     }
     const int blocks = total_items < max_blocks ? total_items : max_blocks;
-    k3c_fast<LI, LJ, LK, V, T, POINT><<<blocks, C::THREADS, 0, s>>>(boys_table, bra, ket, map, omega, out,
-                                                                    counter, total_items);
+    k3c_fast<LI, LJ, LK, V, T, POINT><<<blocks, C::THREADS, smem, s>>>(boys_table, bra, ket, map, omega, out,
+                                                                       counter, total_items);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 

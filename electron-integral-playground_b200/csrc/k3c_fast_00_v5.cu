@@ -1,0 +1,19 @@
+// Fast (mu nu|P) instances for (l_i, l_j) = (0, 0), l_k = 0..4, tuning variant 5.
+#include "k3c_fast.cuh"
+
+namespace eip {
+
+int launch_fast3c_00_v5(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket,
+                           const BatchMap& map, int total_items, double omega, double* out, int* counter,
+                           cudaStream_t s) {
+    switch (lk) {
+        case 0: return launch_one<0, 0, 0, 5, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 1: return launch_one<0, 0, 1, 5, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 2: return launch_one<0, 0, 2, 5, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 3: return launch_one<0, 0, 3, 5, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 4: return launch_one<0, 0, 4, 5, double>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+    }
+    return 1;
+}
+
+}  // namespace eip

@@ -3,17 +3,21 @@
 A request is one molecule (its pair and auxiliary tables, the C-ABI formats)
 asking for S, V, (P|Q) and (mu nu|P).  The server
 
-* splits each request into device pieces: (mu nu|P) in slices of auxiliary
-  shells small enough for the HBM budget (a 200-atom molecule's packed
-  (mu nu|P) alone is ~650 GB), (P|Q) (the one-centre metric as pair classes
-  (0, l_P), `batch.metric_pair_tables`), and V (the pair tables with the
-  nuclei as point-charge ket);
+* splits each request into device pieces: (mu nu|P) with V (one slot: the
+  pair tables against the auxiliary basis and against the nuclei as
+  point-charge ket) and (P|Q) (the one-centre metric as pair classes
+  (0, l_P), `batch.metric_pair_tables`).  A (mu nu|P) too large for one piece
+  (a 200-atom molecule's packed (mu nu|P) alone is ~580 GB) becomes windows of
+  auxiliary shells over ONE resident batch of the request (V in its first
+  window): its tables are built and uploaded once and stay on the device until
+  its last window retires;
 * admits pieces in arrival order whenever the device arena (one allocation of
   `budget_bytes`, first-fit sub-allocated) has room for their packed output,
   so requests that arrive while others run are admitted as memory frees up;
-* batches every piece admitted at one moment into ONE batch (one CUDA-graph
-  launch over all their classes) on its own stream; up to `max_inflight`
-  launches overlap on the device;
+* batches the whole pieces admitted at one moment into ONE batch (one
+  CUDA-graph launch over all their classes) on its own stream, and launches a
+  window alone on its request's resident batch; up to `max_inflight` launches
+  overlap on the device;
 * when a launch completes, hands each of its pieces' packed class blocks
   (device views into the arena) to `consumer(request, piece, blocks)` (default:
   a per-request digest, sum of squares, on the device) and frees the launch's
@@ -21,11 +25,12 @@ asking for S, V, (P|Q) and (mu nu|P).  The server
   while the GPU works.
 
 Latency of a request = completion of its last piece minus its arrival.
-Precision "mixed" uses the batch's FP32 gate (<= 1e-10 of FP64, tested);
-V is always FP64.
+Precision "mixed" uses the batch's FP32 gate for (mu nu|P) (<= 1e-10 of FP64,
+tested); V and (P|Q) are always FP64.
 """
 
 import collections
+import concurrent.futures
 import queue
 import threading
 import time
@@ -70,15 +75,39 @@ def _n_shell_pairs(p):
     return len(np.unique(key))
 
 
-def packed_elems(pair_data, aux_data, n_charge=0):
-    """Doubles of the packed spherical output of one molecule slot."""
+def packed_elems(pair_data, aux_data, n_charge=0, n_sp=None):
+    """Doubles of the packed spherical output of one molecule slot (n_sp: the
+    shell-pair count per pair class, if already known)."""
     total = 0
     n_aux_sh = {l: len(np.unique(np.asarray(a.i_ao_start))) for l, a in aux_data.items()}
     for (li, lj), p in pair_data.items():
-        n_sp = _n_shell_pairs(p)
+        nsp = n_sp[(li, lj)] if n_sp is not None else _n_shell_pairs(p)
         for lk, nax in n_aux_sh.items():
-            total += n_sp * (2 * li + 1) * (2 * lj + 1) * (2 * lk + 1) * nax
-        total += n_sp * (2 * li + 1) * (2 * lj + 1) * n_charge
+            total += nsp * (2 * li + 1) * (2 * lj + 1) * (2 * lk + 1) * nax
+        total += nsp * (2 * li + 1) * (2 * lj + 1) * n_charge
+    return total
+
+
+def window_edges(aux_data, n_aux, max_functions):
+    """Auxiliary-function edges of windows of whole shells, at most
+    max_functions functions each (one shell at least)."""
+    starts = np.unique(np.concatenate([np.asarray(a.i_ao_start) for a in aux_data.values()]))
+    edges = [0]
+    for s in starts:
+        if s - edges[-1] >= max_functions:
+            edges.append(int(s))
+    edges.append(n_aux)
+    return edges
+
+
+def window_elems(pair_sp, aux_starts, lo, hi):
+    """Doubles of the packed output of the auxiliary window [lo, hi).
+    pair_sp: {(l_i, l_j): shell pairs}; aux_starts: {l_k: sorted shell starts}."""
+    total = 0
+    for lk, st in aux_starts.items():
+        nax = int(np.searchsorted(st, hi) - np.searchsorted(st, lo))
+        for (li, lj), nsp in pair_sp.items():
+            total += nsp * (2 * li + 1) * (2 * lj + 1) * (2 * lk + 1) * nax
     return total
 
 
@@ -93,18 +122,26 @@ class Request:
         self.digest = 0.0
         self.done = None
         self.S = None
+        self.resident = None  # the resident batch of a windowed request (or its pending build)
+        self.windows_left = 0
+        self.charges = None
 
 
 class Piece:
-    """One molecule slot of a batch: kind "3c" (an auxiliary slice starting at
-    function aux_lo), "metric" (rows of (P|Q) from aux_lo) or "V"."""
+    """One molecule slot of a batch: kind "3c" ((mu nu|P) of the auxiliary
+    shells from function aux_lo, with V when it carries the charges; a window
+    of the request's resident batch when window is set) or "metric" (columns
+    of (P|Q) from function aux_lo)."""
 
-    def __init__(self, request, kind, pair_data, aux_data, aux_lo, elems, charges=None):
+    def __init__(self, request, kind, pair_data, aux_data, aux_lo, elems, charges=None, aux_hi=None,
+                 window=False):
         self.request = request
         self.kind = kind
         self.pair_data = pair_data
         self.aux_data = aux_data
         self.aux_lo = aux_lo
+        self.aux_hi = aux_hi
+        self.window = window  # computed as a window of the request's resident batch
         self.elems = elems
         self.charges = charges
 
@@ -155,9 +192,10 @@ class Arena:
 
 
 def default_consumer(request, piece, blocks):
-    """blocks: [((l_i, l_j, l_k), device view of the packed block)] of one piece."""
-    for _, v in blocks:
-        request.digest += float((v * v).sum())
+    """blocks: [((l_i, l_j, l_k), device view of the packed block)] of one piece;
+    adds the sum of squares of every value (one read of each block)."""
+    if blocks:
+        request.digest += float(sum(v.dot(v) for _, v in blocks))
 
 
 class IntegralServer:
@@ -176,6 +214,11 @@ class IntegralServer:
         self.keep_blocks = keep_blocks
         self.kept = collections.defaultdict(dict)
         self.launches = 0
+        # finished batches: destroyed only while nothing is in flight, because
+        # freeing device memory synchronises the whole device
+        self._dead = []
+        # host seconds spent planning pieces, building batches, retiring launches
+        self.host_s = {"plan": 0.0, "build": 0.0, "retire": 0.0}
 
     # -- request decomposition -------------------------------------------------
     def _sliced(self, req, kind, pair_data):
@@ -189,15 +232,34 @@ class IntegralServer:
 
     def pieces_of(self, req):
         mol = req.molecule
-        out = self._sliced(req, "3c", req.pair_data)
-        out += self._sliced(req, "metric", metric_pair_tables(req.aux_data))
+        pair_sp = {k: _n_shell_pairs(p) for k, p in req.pair_data.items()}
         charges = np.asarray(mol.geometry, np.float64).reshape(-1, 3)
-        out.append(Piece(req, "V", req.pair_data, {}, 0, packed_elems(req.pair_data, {}, len(charges)),
-                         charges=charges))
+        v_elems = packed_elems(req.pair_data, {}, len(charges), n_sp=pair_sp)
+        full = packed_elems(req.pair_data, req.aux_data, n_sp=pair_sp)
+        if full + v_elems <= self.slice_elems:
+            out = [Piece(req, "3c", req.pair_data, req.aux_data, 0, full + v_elems, charges=charges)]
+        else:
+            req.charges = charges
+            starts = {l: np.unique(np.asarray(a.i_ao_start)) for l, a in req.aux_data.items()}
+            width = max(1, int(self.slice_elems / ((full + v_elems) / mol.n_aux)))
+            edges = window_edges(req.aux_data, mol.n_aux, width)
+            out = [Piece(req, "3c", req.pair_data, req.aux_data, lo,
+                         window_elems(pair_sp, starts, lo, hi) + (v_elems if k == 0 else 0),
+                         charges=charges if k == 0 else None, aux_hi=hi, window=True)
+                   for k, (lo, hi) in enumerate(zip(edges[:-1], edges[1:]))]
+            req.windows_left = len(out)
+        out += self._sliced(req, "metric", metric_pair_tables(req.aux_data))
         for p in out:
             if p.elems > self.arena.capacity:
                 raise ValueError(f"request {req.rid}: one auxiliary shell slice exceeds the HBM budget")
         return out
+
+    def _build_resident(self, req, device):
+        """Resident batch of a windowed request (runs on the builder thread)."""
+        self.torch.cuda.set_device(device)
+        kw = {} if self.fp32_threshold is None else {"fp32_threshold": self.fp32_threshold}
+        return ThreeCenterBatch([req.molecule], [req.pair_data], [req.aux_data], precision=self.precision,
+                                charges_list=[req.charges], **kw)
 
     # -- S on a worker thread ----------------------------------------------------
     def _host_worker(self, q):
@@ -220,6 +282,10 @@ class IntegralServer:
         worker = threading.Thread(target=self._host_worker, args=(hostq,), daemon=True)
         if self.host_overlap:
             worker.start()
+        # resident batches of windowed requests are built on a builder thread
+        # as the requests arrive, overlapping the loop and the GPU
+        builder = concurrent.futures.ThreadPoolExecutor(max_workers=1)
+        device = self.torch.cuda.current_device()
         t0 = time.perf_counter()
         finished = []
         n_total = len(todo)
@@ -230,25 +296,46 @@ class IntegralServer:
                     req = todo.popleft()
                     if not realtime:
                         req.arrival = now
+                    tp = time.perf_counter()
                     ps = self.pieces_of(req)
+                    self.host_s["plan"] += time.perf_counter() - tp
                     req.pieces_left = len(ps)
+                    if req.windows_left:
+                        req.resident = builder.submit(self._build_resident, req, device)
                     waiting.extend(ps)
                     if self.host_overlap:
                         hostq.put(req)
                 for item in list(inflight):
                     if item[1].query():
+                        tr = time.perf_counter()
                         self._retire(item, finished, t0)
+                        self.host_s["retire"] += time.perf_counter() - tr
                         inflight.remove(item)
+                if self._dead and (not inflight or len(self._dead) > 64):
+                    for b in self._dead:
+                        b.close()
+                    self._dead.clear()
                 if waiting and len(inflight) < self.max_inflight:
                     largest = self.arena.largest_free
                     group, total = [], 0
-                    while waiting and total + waiting[0].elems + 32 * (len(group) + 1) <= largest:
-                        p = waiting.popleft()
-                        group.append(p)
-                        total += p.elems
+                    if waiting[0].window:
+                        if waiting[0].elems + 32 <= largest:
+                            group.append(waiting.popleft())
+                            total = group[0].elems
+                    else:
+                        while (waiting and not waiting[0].window
+                               and total + waiting[0].elems + 32 * (len(group) + 1) <= largest):
+                            p = waiting.popleft()
+                            group.append(p)
+                            total += p.elems
                     if group:
                         off, alloc = self.arena.alloc(total + 32 * len(group))
-                        inflight.append(self._launch(group, off, alloc))
+                        tb = time.perf_counter()
+                        if group[0].window:
+                            inflight.append(self._launch_window(group[0], off, alloc))
+                        else:
+                            inflight.append(self._launch(group, off, alloc))
+                        self.host_s["build"] += time.perf_counter() - tb
                         continue
                     if not inflight:
                         raise RuntimeError("a piece does not fit the empty arena")
@@ -259,7 +346,17 @@ class IntegralServer:
         finally:
             for item in inflight:
                 item[0].sync()
+            for item in inflight:
                 item[0].close()
+            for b in self._dead:
+                b.close()
+            self._dead.clear()
+            builder.shutdown(wait=True)
+            for r in requests:
+                if r.resident is not None:
+                    b = r.resident.result() if isinstance(r.resident, concurrent.futures.Future) else r.resident
+                    b.close()
+                    r.resident = None
             if self.host_overlap:
                 hostq.put(None)
                 worker.join()
@@ -267,7 +364,8 @@ class IntegralServer:
         lat = np.array([r.done - r.arrival for r in finished])
         return {"requests": n_total, "wall_s": wall, "throughput_rps": n_total / wall,
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-                "latency_mean_s": float(lat.mean()), "launches": self.launches}
+                "latency_mean_s": float(lat.mean()), "launches": self.launches,
+                "host_s": {k: round(v, 3) for k, v in self.host_s.items()}}
 
     def _launch(self, group, off, alloc):
         """One batch (one CUDA-graph launch) over every piece of the group, its
@@ -285,23 +383,50 @@ class IntegralServer:
         ev = torch.cuda.Event()
         ev.record(torch.cuda.ExternalStream(b.stream))
         self.launches += 1
-        return (b, ev, group, off, alloc)
+        layout = [self._layout(p, lambda li, lj, lk, m=m: b.block(m, li, lj, lk)) for m, p in enumerate(group)]
+        return (b, ev, group, off, alloc, layout)
+
+    def _launch_window(self, piece, off, alloc):
+        """One auxiliary window of a large request on its resident batch (built
+        and uploaded at the first window)."""
+        torch = self.torch
+        req = piece.request
+        if isinstance(req.resident, concurrent.futures.Future):
+            req.resident = req.resident.result()
+        b = req.resident
+        n = b.window([piece.aux_lo], [piece.aux_hi], with_charges=piece.charges is not None)
+        if n != piece.elems:
+            raise RuntimeError("window output size differs from the planned size")
+        layout = [self._layout(piece, lambda li, lj, lk: b.window_block(0, li, lj, lk))]
+        b.run_window(self.arena.buf.data_ptr() + 8 * off)
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.ExternalStream(b.stream))
+        self.launches += 1
+        return (b, ev, [piece], off, alloc, layout)
+
+    @staticmethod
+    def _layout(piece, block_of):
+        """[(class, offset, length)] of a piece's blocks in its launch's output."""
+        out = []
+        for li, lj, lk in piece.classes():
+            blk = block_of(li, lj, lk)
+            if blk is None:
+                continue
+            o, nsp, nax = blk
+            out.append(((li, lj, lk), o, nsp * (2 * li + 1) * (2 * lj + 1) * (2 * max(lk, 0) + 1) * nax))
+        return out
 
     def _retire(self, item, finished, t0):
-        batch, _, pieces, off, alloc = item
-        batch.status()
-        # the consumer's kernels run on torch's current stream: order them after the batch
+        batch, _, pieces, off, alloc, layout = item
+        windowed = pieces[0].window
+        if not windowed:
+            batch.status()
+        # the launch's completion event has been seen, so the consumer's kernels
+        # (torch's current stream) read finished output; no stream wait (a
+        # windowed batch's stream may already hold its next window)
         torch = self.torch
-        torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(batch.stream))
-        for m, p in enumerate(pieces):
-            blocks = []
-            for li, lj, lk in p.classes():
-                blk = batch.block(m, li, lj, lk)
-                if blk is None:
-                    continue
-                o, nsp, nax = blk
-                n = nsp * (2 * li + 1) * (2 * lj + 1) * (2 * max(lk, 0) + 1) * nax
-                blocks.append(((li, lj, lk), self.arena.buf[off + o:off + o + n]))
+        for p, lay in zip(pieces, layout):
+            blocks = [(c, self.arena.buf[off + o:off + o + n]) for c, o, n in lay]
             self.consumer(p.request, p, blocks)
             if self.keep_blocks:
                 for c, v in blocks:
@@ -316,5 +441,13 @@ class IntegralServer:
         ev.record(torch.cuda.current_stream())
         ev.synchronize()
         self.arena.release(off, alloc)
-        batch.bind_output(0)
-        batch.close()
+        if windowed:
+            req = pieces[0].request
+            req.windows_left -= 1
+            if req.windows_left == 0:  # its last window: check every window's self-checks, free the tables
+                batch.status()
+                self._dead.append(batch)
+                req.resident = None
+        else:
+            batch.bind_output(0)
+            self._dead.append(batch)

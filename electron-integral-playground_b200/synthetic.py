@@ -210,3 +210,42 @@ def config1_batch(seed: int = 0, n_molecule: int = 64):
     sizes = molecule_sizes(n_molecule, 3, 60, seed)
     return [attach_synthetic_basis(organic_molecule(n, seed * 1000 + i), aux_l_max=4, seed=seed)
             for i, n in enumerate(sizes)]
+
+
+def random_shell_triplet(rng, l_orbital_max=4, l_aux_max=5, max_primitives=8, box_angstrom=6.0,
+                         exponent_range=(0.05, 1e4)):
+    """One random shell triplet (l_i <= l_j | l_k): centres uniform in a cube,
+    1..max_primitives primitives per shell, exponents log-uniform, coefficients
+    uniform in [0.1, 1].  Returns ((l_i, l_j), pair table, l_k, aux table,
+    molecule stub with n_ao = n_i + n_j and n_aux = n_k, spherical)."""
+    from .data_structure import PrimitivePairData
+
+    li, lj = (int(x) for x in sorted(rng.integers(0, l_orbital_max + 1, size=2)))
+    lk = int(rng.integers(0, l_aux_max + 1))
+    A, B, C = rng.uniform(0, box_angstrom, size=(3, 3)) * angstrom_to_bohr
+    npi, npj, npk = (int(x) for x in rng.integers(1, max_primitives + 1, size=3))
+    lo, hi = np.log(exponent_range[0]), np.log(exponent_range[1])
+    ea, eb, ek = (np.exp(rng.uniform(lo, hi, n)) for n in (npi, npj, npk))
+    ca, cb, ck = rng.uniform(0.1, 1, npi), rng.uniform(0.1, 1, npj), rng.uniform(0.1, 1, npk)
+    a, b = np.repeat(ea, npj), np.tile(eb, npi)
+    p = a + b
+    P = (a[:, None] * A + b[:, None] * B) / p[:, None]
+    coef = np.repeat(ca, npj) * np.tile(cb, npi) * np.exp(-a * b / p * np.sum((A - B) ** 2))
+    n_i, n_k = 2 * li + 1, 2 * lk + 1
+    pair = PrimitivePairData(P_p=np.ascontiguousarray(np.c_[P, p]),
+                             A_a=np.ascontiguousarray(np.c_[np.tile(A, (len(a), 1)), a]),
+                             B_b=np.ascontiguousarray(np.c_[np.tile(B, (len(a), 1)), b]), coefficient=coef,
+                             i_ao_start=np.zeros(len(a), np.int32), j_ao_start=np.full(len(a), n_i, np.int32),
+                             i_atom=None, j_atom=None)
+    aux = PrimitivePairData(P_p=None, A_a=np.ascontiguousarray(np.c_[np.tile(C, (npk, 1)), ek]), B_b=None,
+                            coefficient=ck, i_ao_start=np.zeros(npk, np.int32), j_ao_start=None, i_atom=None,
+                            j_atom=None)
+    mol = Molecule(elements=[], geometry=np.zeros((0, 3)), n_ao=n_i + 2 * lj + 1, n_aux=n_k, spherical_basis=True)
+    return (li, lj), pair, lk, aux, mol
+
+
+def config3_triplets(seed: int = 0, n: int = 2000):
+    """2000 random shell triplets: centres in a 6 A cube, orbital l <= 4,
+    auxiliary l <= 5, 1-8 primitives, exponents log-uniform in [0.05, 1e4]."""
+    rng = np.random.default_rng(seed + 3)
+    return [random_shell_triplet(rng) for _ in range(n)]

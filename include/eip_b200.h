@@ -79,7 +79,7 @@ unsigned long long eip_kernel_launch_count(void);
  * last reference-ABI call, in milliseconds. */
 float eip_last_kernel_ms(void);
 
-/* Tuning variant (0..3) of the fast (mu nu|P) kernel of class (i_L, j_L | k_L),
+/* Tuning variant (0..5) of the fast (mu nu|P) kernel of class (i_L, j_L | k_L),
  * i_L <= j_L <= 2 or (i_L, j_L) = (0, 3), (0, 4), k_L <= 4: accumulator budget and register cap (see
  * k3c_fast.cuh).  Affects launches made after the call (a batch's graph keeps
  * the variants it was captured with).  set returns 1 for an invalid
@@ -166,6 +166,22 @@ int eip_batch_run(eip_batch* batch, int checksum);
 /* Launch the kernels of one (i_L, j_L | k_L) class alone, on the batch stream,
  * outside the graph (per-kernel timing); returns 1 if the class is absent. */
 int eip_batch_run_class(eip_batch* batch, int i_L, int j_L, int k_L);
+/* Auxiliary-window runs: compute only the auxiliary shells whose first
+ * function lies in [fn_lo[m], fn_hi[m]) for molecule m (NULL arrays: all),
+ * reusing the batch's resident tables (a molecule whose whole output does not
+ * fit device memory is computed window by window without rebuilding them).
+ * window_plan sets the window and returns its packed output size in doubles
+ * (-1 on error); point-charge classes are included only with with_charges.
+ * The window's layout is the batch layout with each molecule's auxiliary
+ * shells restricted to the window, blocks at eip_batch_window_block()'s
+ * offsets.  run_window launches it (direct launches, not the graph) on the
+ * batch stream into device_output.  Runs of one batch execute in order; the
+ * window maps cycle through 4 slots, so a window_plan waits (on the host) only
+ * while the run planned 4 windows earlier has not started. */
+long long eip_batch_window_plan(eip_batch* batch, const int* fn_lo, const int* fn_hi, int with_charges);
+int eip_batch_window_block(eip_batch* batch, int molecule, int i_L, int j_L, int k_L, long long* offset,
+                           int* n_pair_shells, int* n_aux_shells);
+int eip_batch_run_window(eip_batch* batch, double* device_output, int checksum);
 int eip_batch_sync(eip_batch* batch);
 /* 0 if every class kernel of the last run passed its self-checks, 3 if one
  * recorded an inconsistency (eip_batch_error names it). */

@@ -60,6 +60,7 @@ def oracle():
         _cache["oracle"] = IntegralLibrary(ORACLE_SO, "oracle_")
         lib = _cache["oracle"].lib
         lib.oracle_boys.argtypes = [ctypes.c_int, ctypes.c_double, _c_double_p]
+        lib.oracle_boys_many.argtypes = [ctypes.c_int, ctypes.c_int, _c_double_p, _c_double_p]
         lib.oracle_spherical_matrix.argtypes = [ctypes.c_int, _c_double_p]
     return _cache["oracle"]
 
@@ -74,6 +75,14 @@ def reference():
 def boys(L, x):
     y = np.empty(L + 1)
     oracle().lib.oracle_boys(int(L), float(x), _dp(y))
+    return y
+
+
+def boys_many(L, xs):
+    """F_m(x), m = 0..L, for every x (long-double series): shape (len(xs), L + 1)."""
+    xs = np.ascontiguousarray(xs, dtype=np.float64)
+    y = np.empty((xs.size, L + 1))
+    oracle().lib.oracle_boys_many(int(L), int(xs.size), _dp(xs), _dp(y))
     return y
 
 

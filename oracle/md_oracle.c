@@ -75,6 +75,11 @@ void oracle_boys(int L, double xd, double* y) {
     for (int m = 0; m <= L; m++) y[m] = (double)F[m];
 }
 
+/* F_m(x[i]), m = 0..L, for n arguments: y[i * (L + 1) + m]. */
+void oracle_boys_many(int L, int n, const double* x, double* y) {
+    for (int i = 0; i < n; i++) oracle_boys(L, x[i], y + (size_t)i * (L + 1));
+}
+
 /* ---- real solid harmonics as polynomials in x, y, z --------------------- */
 typedef struct { long double c[10][10][10]; } poly3;
 

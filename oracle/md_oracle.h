@@ -48,6 +48,7 @@ int oracle_overlap(int i_L, int j_L, const double* pair_A_a, const double* pair_
 
 /* F_m(x) for m = 0..L into y[0..L] (long-double series; reference for the device Boys). */
 void oracle_boys(int L, double x, double* y);
+void oracle_boys_many(int L, int n, const double* x, double* y);
 
 /* Real-solid-harmonic coefficients P_l[m][c] (row-major, (2l+1) x (l+1)(l+2)/2). */
 void oracle_spherical_matrix(int l, double* out);

@@ -84,7 +84,7 @@ def test_every_tuning_variant_matches_reference(small_batch):
     want = oracle.drive_three_center(ref, pds[3], ads[3], mols[3])
     saved = {(li, lj, lk): L.eip_tune_get(li, lj, lk) for (li, lj) in pds[3] for lk in ads[3]}
     try:
-        for v in range(4):
+        for v in range(6):
             for (li, lj, lk) in saved:
                 if saved[(li, lj, lk)] >= 0:
                     L.eip_tune_set(li, lj, lk, v)
@@ -179,8 +179,9 @@ def test_batch_metric_matches_two_center(small_batch, omega):
     b.close()
 
 
-def test_mixed_metric_within_1e10_of_fp64():
-    """The FP32 gate on one-centre (metric) pairs uses the auxiliary bound."""
+def test_mixed_batch_keeps_the_metric_fp64():
+    """(P|Q) feeds a Cholesky factorisation: in a mixed-precision batch its
+    one-centre pairs never take the FP32 path, so it equals the FP64 batch."""
     m = _two_fragments()
     ad = pu.form_auxiliary_pair_data(m)
     metric = bt.metric_pair_tables(ad)
@@ -190,7 +191,59 @@ def test_mixed_metric_within_1e10_of_fp64():
         b.alloc_output()
         b.run()
         b.status()
-    err = np.max(np.abs(f64.dense_metric(0) - mix.dense_metric(0)))
-    assert err <= 1e-10, err
+    assert all(mix.precision_split(0, l, k)[1] == 0 for l in ad for k in ad)
+    np.testing.assert_array_equal(f64.dense_metric(0), mix.dense_metric(0))
     f64.close()
     mix.close()
+
+
+def test_window_runs_reproduce_the_full_run(small_batch):
+    """Runs over auxiliary windows (per-molecule function ranges, resident
+    tables) give exactly the corresponding slices of the full run's blocks,
+    FP64 and mixed, with and without the point-charge class."""
+    import torch
+
+    mols, pds, ads, _ = small_batch
+    charges = [m.geometry for m in mols]
+    for precision in ("fp64", "mixed"):
+        b = bt.ThreeCenterBatch(mols, pds, ads, precision=precision, charges_list=charges)
+        b.alloc_output()
+        b.run()
+        b.status()
+        full = np.empty(b.output_elems)
+        b._check(b.L.eip_batch_copy_output(b.h, 0, b.output_elems, full.ctypes.data_as(
+            __import__("ctypes").POINTER(__import__("ctypes").c_double))), "copy")
+        rng = np.random.default_rng(3)
+        for trial in range(3):
+            lo = np.array([int(rng.integers(0, max(1, m.n_aux // 2))) for m in mols])
+            hi = np.array([int(rng.integers(l + 1, m.n_aux + 1)) for l, m in zip(lo, mols)])
+            if trial == 2:
+                lo[1], hi[1] = 0, 0  # an empty window
+            n = b.window(lo, hi, with_charges=(trial == 0))
+            out = torch.full((max(n, 1),), float("nan"), dtype=torch.float64, device="cuda")
+            b.run_window(out.data_ptr())
+            b.sync()
+            b.status()
+            w = out.cpu().numpy()
+            seen = 0
+            for m in range(len(mols)):
+                for (li, lj) in pds[m]:
+                    kets = list(ads[m]) + [bt.POINT_CHARGES]
+                    for lk in kets:
+                        f_off, nsp, nax = b.block(m, li, lj, lk)
+                        w_off, wsp, wax = b.window_block(m, li, lj, lk)
+                        nk = 1 if lk == bt.POINT_CHARGES else 2 * lk + 1
+                        shape = (nsp, 2 * li + 1, 2 * lj + 1, nk)
+                        fb = full[f_off:f_off + np.prod(shape) * nax].reshape(shape + (nax,))
+                        if lk == bt.POINT_CHARGES:
+                            sel = slice(0, nax) if trial == 0 else slice(0, 0)
+                        else:
+                            st = np.unique(np.asarray(ads[m][lk].i_ao_start))
+                            sel = slice(int(np.searchsorted(st, lo[m])), int(np.searchsorted(st, hi[m])))
+                        want = fb[..., sel]
+                        assert wsp == nsp and wax == want.shape[-1]
+                        got = w[w_off:w_off + want.size].reshape(want.shape)
+                        assert np.array_equal(got, want), (precision, m, li, lj, lk)
+                        seen += want.size
+            assert seen == n
+        b.close()

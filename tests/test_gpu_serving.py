@@ -56,32 +56,39 @@ def test_request_alone_equals_request_in_the_mix():
         np.testing.assert_array_equal(r.S, mi.overlap(r.pair_data, r.molecule))
 
 
-def test_served_blocks_match_drop_in():
-    """The served V blocks and (P|Q) rows equal the drop-in entry points."""
+@pytest.mark.parametrize("budget", [160e6, 6e6])
+def test_served_blocks_match_drop_in(budget):
+    """The served V blocks and (P|Q) columns equal the drop-in entry points,
+    whole (160 MB arena) and as windows / slices (6 MB arena)."""
     r = _requests([6])[0]
-    s = sv.IntegralServer(budget_bytes=64e6, precision="fp64", keep_blocks=True, host_overlap=False)
+    s = sv.IntegralServer(budget_bytes=budget, precision="fp64", keep_blocks=True, host_overlap=False)
     s.serve([r], realtime=False)
     kept = s.kept[r.rid]
     mol = r.molecule
     V = mi.nuclear_attraction(r.pair_data, mol, mol.geometry)
     M = mi.two_center(r.aux_data, mol)
     nc = mol.geometry.shape[0]
+    windows = {k[1] for k in kept if k[0] == "3c"}
+    assert (len(windows) > 1) == (budget < 1e7)
     for (li, lj), p in r.pair_data.items():
         pairs = np.unique(np.stack([np.asarray(p.i_ao_start), np.asarray(p.j_ao_start)], 1), axis=0)
-        blk = kept[("V", 0, li, lj, sv.POINT_CHARGES)].reshape(len(pairs), 2 * li + 1, 2 * lj + 1, nc)
+        blk = kept[("3c", 0, li, lj, sv.POINT_CHARGES)].reshape(len(pairs), 2 * li + 1, 2 * lj + 1, nc)
         for t, (i0, j0) in enumerate(pairs):
             np.testing.assert_allclose(blk[t], V[i0:i0 + 2 * li + 1, j0:j0 + 2 * lj + 1, :], rtol=0, atol=1e-13)
-    n_seen = 0
+    n_cols = 0
     for key, v in kept.items():
         if key[0] != "metric":
             continue
         _, lo, _, lP, lQ = key
         P0 = np.unique(np.asarray(r.aux_data[lP].i_ao_start))
-        Q0 = np.unique(np.asarray(r.aux_data[lQ].i_ao_start))
-        blk = v.reshape(len(P0), 2 * lP + 1, 2 * lQ + 1, len(Q0))
+        nP, nQ = 2 * lP + 1, 2 * lQ + 1
+        nax = v.size // (len(P0) * nP * nQ)
+        allQ = np.unique(np.asarray(r.aux_data[lQ].i_ao_start))
+        Q0 = allQ[allQ >= lo][:nax]
+        blk = v.reshape(len(P0), nP, nQ, nax)
         for s_, p0 in enumerate(P0):
-            ref = M[p0:p0 + 2 * lP + 1][:, Q0[:, None] + np.arange(2 * lQ + 1)[None, :]]
+            ref = M[p0:p0 + nP][:, Q0[:, None] + np.arange(nQ)[None, :]]
             np.testing.assert_allclose(blk[s_], ref.transpose(0, 2, 1), rtol=0,
                                        atol=max(1e-12, 1e-13 * float(np.abs(ref).max())))
-            n_seen += 1
-    assert n_seen > 0
+        n_cols += nax * nQ
+    assert n_cols == M.shape[0] * len(r.aux_data)  # every column once per l_P
