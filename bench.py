@@ -414,8 +414,15 @@ def main():
     tuning = at.load()
     if args.tune:
         table, timings = at.tune(batch, sorted(per_class))
+        # FP32 kernels: a mixed batch whose every shell pair takes the FP32 path
+        all32 = bt.ThreeCenterBatch(mols, pds, ads, precision="mixed", fp32_threshold=float("inf"))
+        all32.bind_output(out_ptr)
+        table32, timings32 = at.tune(all32, sorted(per_class), fp32=True)
+        all32.bind_output(0)
+        all32.close()
         at.save(table, timings, {"workload": WORKLOAD, "seed": args.seed, "molecules": args.molecules,
-                                 "gpu": torch.cuda.get_device_name(local)})
+                                 "gpu": torch.cuda.get_device_name(local)}, table_fp32=table32,
+                timings_fp32=timings32)
         tuning = at.load()
     mixed = bt.ThreeCenterBatch(mols, pds, ads, precision="mixed", fp32_threshold=args.fp32_threshold)
     mixed.bind_output(out_ptr)  # same layout; the two paths run one after the other

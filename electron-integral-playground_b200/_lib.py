@@ -48,6 +48,10 @@ def lib():
         L.eip_tune_set.restype = c_int
         L.eip_tune_get.argtypes = [c_int, c_int, c_int]
         L.eip_tune_get.restype = c_int
+        L.eip_tune_set_fp32.argtypes = [c_int, c_int, c_int, c_int]
+        L.eip_tune_set_fp32.restype = c_int
+        L.eip_tune_get_fp32.argtypes = [c_int, c_int, c_int]
+        L.eip_tune_get_fp32.restype = c_int
         L.eip_boys.argtypes = [c_int, _dp, c_int, _dp]
         L.eip_boys.restype = c_int
         _lib = L

@@ -18,6 +18,8 @@ int launch_boys_probe(int L, const double* dT, int n, double* dout, cudaStream_t
 bool fast3c_supported(int li, int lj, int lk);
 int fast3c_variant(int li, int lj, int lk);
 int fast3c_set_variant(int li, int lj, int lk, int v);
+int fast3c_variant_fp32(int li, int lj, int lk);
+int fast3c_set_variant_fp32(int li, int lj, int lk, int v);
 size_t e_table_doubles(int li, int lj);
 int launch_e_table(int li, int lj, const BraTable& bra, double* prim_E, cudaStream_t s);
 int launch_fast_point(int li, int lj, const BraTable& bra, const KetTable& ket, const BatchMap& map,

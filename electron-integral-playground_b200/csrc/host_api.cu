@@ -388,6 +388,12 @@ int eip_tune_set(int i_L, int j_L, int k_L, int variant) { return fast3c_set_var
 
 int eip_tune_get(int i_L, int j_L, int k_L) { return fast3c_variant(i_L, j_L, k_L); }
 
+int eip_tune_set_fp32(int i_L, int j_L, int k_L, int variant) {
+    return fast3c_set_variant_fp32(i_L, j_L, k_L, variant);
+}
+
+int eip_tune_get_fp32(int i_L, int j_L, int k_L) { return fast3c_variant_fp32(i_L, j_L, k_L); }
+
 int eip_boys(int L, const double* T, int n, double* F) {
     Context& c = ctx();
     std::lock_guard<std::mutex> lock(c.mu);

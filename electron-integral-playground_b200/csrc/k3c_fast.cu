@@ -10,22 +10,30 @@ namespace eip {
     int launch_fast3c_##I##J##_v##V(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket, \
                                     const BatchMap& map, int total_items, double omega, double* out,         \
                                     int* counter, cudaStream_t s);
+#define EIP_DECL_F(I, J, V)                                                                                     \
+    int launch_fast3c_##I##J##_f32_v##V(int lk, const double* boys_table, const BraTable& bra,                 \
+                                        const KetTable& ket, const BatchMap& map, int total_items, double omega, \
+                                        double* out, int* counter, cudaStream_t s);
 #define EIP_DECL(I, J)                                                                                      \
     EIP_DECL_V(I, J, 0) EIP_DECL_V(I, J, 1) EIP_DECL_V(I, J, 2) EIP_DECL_V(I, J, 3) EIP_DECL_V(I, J, 4)     \
     EIP_DECL_V(I, J, 5)                                                                                     \
     int launch_fast3c_##I##J##_f32(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket, \
                                    const BatchMap& map, int total_items, double omega, double* out,         \
                                    int* counter, cudaStream_t s);                                           \
+    EIP_DECL_F(I, J, 2) EIP_DECL_F(I, J, 3) EIP_DECL_F(I, J, 4)                                              \
     int launch_e_table_##I##J(const BraTable& bra, double* prim_E, cudaStream_t s);
 EIP_DECL(0, 0) EIP_DECL(0, 1) EIP_DECL(1, 1) EIP_DECL(0, 2) EIP_DECL(1, 2) EIP_DECL(2, 2) EIP_DECL(0, 3) EIP_DECL(0, 4)
 #undef EIP_DECL
 #undef EIP_DECL_V
+#undef EIP_DECL_F
 
 // Fast pair classes: l_i <= l_j <= 2 (orbital shell pairs) and (0, 3), (0, 4)
 // (a one-centre bra: the two-centre metric (P|Q) as pair class (0, l_P) with
 // A = B = P).  Variant per (l_i, l_j, l_k), default 0; the autotuner's choices
 // on B200 (tuning/b200_fp64.json) are applied with eip_tune_set.
 static int g_variant[5][5][5] = {};
+// FP32 (mixed-precision) kernels: compiled variants 0, 2, 3, 4; default 0.
+static int g_variant32[5][5][5] = {};
 
 bool fast3c_supported(int li, int lj, int lk) {
     const bool pair_ok = li >= 0 && li <= lj && (lj <= 2 || (li == 0 && lj <= 4));
@@ -42,6 +50,16 @@ int fast3c_set_variant(int li, int lj, int lk, int v) {
     return 0;
 }
 
+int fast3c_variant_fp32(int li, int lj, int lk) {
+    return fast3c_supported(li, lj, lk) ? g_variant32[li][lj][lk] : -1;
+}
+
+int fast3c_set_variant_fp32(int li, int lj, int lk, int v) {
+    if (!fast3c_supported(li, lj, lk) || !(v == 0 || v == 2 || v == 3 || v == 4)) return 1;
+    g_variant32[li][lj][lk] = v;
+    return 0;
+}
+
 size_t e_table_doubles(int li, int lj) {
     size_t n = 0;
     for (int i = 0; i <= li; i++)
@@ -53,7 +71,7 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
                   int total_items, double omega, double* out, int* counter, cudaStream_t s, bool fp32) {
     if (!fast3c_supported(li, lj, lk)) return 1;
     const double* t = boys_table_device();
-    const int v = fp32 ? -1 : g_variant[li][lj][lk];
+    const int v = fp32 ? -1 - g_variant32[li][lj][lk] : g_variant[li][lj][lk];
 #define EIP_GO_V(I, J, V) return launch_fast3c_##I##J##_v##V(lk, t, bra, ket, map, total_items, omega, out, counter, s)
 #define EIP_GO(I, J)                                                                                          \
     switch (v) {                                                                                              \
@@ -63,6 +81,9 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
         case 4: EIP_GO_V(I, J, 4);                                                                            \
         case 5: EIP_GO_V(I, J, 5);                                                                            \
         case -1: return launch_fast3c_##I##J##_f32(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
+        case -3: return launch_fast3c_##I##J##_f32_v2(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
+        case -4: return launch_fast3c_##I##J##_f32_v3(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
+        case -5: return launch_fast3c_##I##J##_f32_v4(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
         default: EIP_GO_V(I, J, 0);                                                                           \
     }
     switch (li * 10 + lj) {

@@ -1,0 +1,20 @@
+// Mixed-precision (FP32 R/ket/bra) (mu nu|P) instances for (l_i, l_j) = (2, 2),
+// l_k = 0..4 (tuning variant 3).
+#include "k3c_fast.cuh"
+
+namespace eip {
+
+int launch_fast3c_22_f32_v3(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket,
+                          const BatchMap& map, int total_items, double omega, double* out, int* counter,
+                          cudaStream_t s) {
+    switch (lk) {
+        case 0: return launch_one<2, 2, 0, 3, float>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 1: return launch_one<2, 2, 1, 3, float>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 2: return launch_one<2, 2, 2, 3, float>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 3: return launch_one<2, 2, 3, 3, float>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+        case 4: return launch_one<2, 2, 4, 3, float>(boys_table, bra, ket, map, total_items, omega, out, counter, s);
+    }
+    return 1;
+}
+
+}  // namespace eip

@@ -86,6 +86,9 @@ float eip_last_kernel_ms(void);
  * class/variant; get returns -1 for a class without fast kernels. */
 int eip_tune_set(int i_L, int j_L, int k_L, int variant);
 int eip_tune_get(int i_L, int j_L, int k_L);
+/* The same for the FP32 kernels of the mixed-precision path: variants 0, 2, 3, 4. */
+int eip_tune_set_fp32(int i_L, int j_L, int k_L, int variant);
+int eip_tune_get_fp32(int i_L, int j_L, int k_L);
 
 /* Device Boys function: F[i*(L+1)+m] = F_m(T[i]), m = 0..L <= 21 (host buffers). */
 int eip_boys(int L, const double* T, int n, double* F);
