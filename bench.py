@@ -57,6 +57,23 @@ def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def shard_seed(seed, rank):
+    """Each rank's molecules: an independent shard of the same generator."""
+    return seed + 1000 * rank
+
+
+def reduce_over_ranks(values, op, device):
+    """All-reduce a list of floats over the process group (identity when alone)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=op)
+    return t.tolist()
+
+
 def build_workload(seed, n_mol):
     import importlib
 
@@ -403,7 +420,7 @@ def main():
     if lm.lib().eip_init(local) != 0:
         raise RuntimeError(lm.lib().eip_last_error().decode())
 
-    mols, pds, ads, stats = build_workload(args.seed + 1000 * rank, args.molecules)
+    mols, pds, ads, stats = build_workload(shard_seed(args.seed, rank), args.molecules)
     tot, per_class = rf.totals(stats)
     batch = bt.ThreeCenterBatch(mols, pds, ads, precision="fp64")
     free, _ = torch.cuda.mem_get_info()
@@ -420,10 +437,11 @@ def main():
         table32, timings32 = at.tune(all32, sorted(per_class), fp32=True)
         all32.bind_output(0)
         all32.close()
-        at.save(table, timings, {"workload": WORKLOAD, "seed": args.seed, "molecules": args.molecules,
-                                 "gpu": torch.cuda.get_device_name(local)}, table_fp32=table32,
-                timings_fp32=timings32)
-        tuning = at.load()
+        if rank == 0:
+            at.save(table, timings, {"workload": WORKLOAD, "seed": args.seed, "molecules": args.molecules,
+                                     "gpu": torch.cuda.get_device_name(local)}, table_fp32=table32,
+                    timings_fp32=timings32)
+        tuning = {"variants": table, "variants_fp32": table32}  # applied in-process by the tuner
     mixed = bt.ThreeCenterBatch(mols, pds, ads, precision="mixed", fp32_threshold=args.fp32_threshold)
     mixed.bind_output(out_ptr)  # same layout; the two paths run one after the other
     table_bytes = {"fp64": batch.table_bytes, "mixed": mixed.table_bytes}
@@ -448,9 +466,7 @@ def main():
         per_step = [marks[k].elapsed_time(marks[k + 1]) for k in range(args.steps)]
         total = marks[0].elapsed_time(marks[-1])
         if world > 1:
-            t = torch.tensor([total], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            total = float(t.item())
+            total = reduce_over_ranks([total], torch.distributed.ReduceOp.MAX, "cuda")[0]
         b.status()
         h_ck = np.empty(len(mols))
 
@@ -472,9 +488,7 @@ def main():
         wall = (time.perf_counter() - t0) * 1e3 / args.steps
         e2e = e0.elapsed_time(e1) / args.steps
         if world > 1:
-            t = torch.tensor([e2e], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e = float(t.item())
+            e2e = reduce_over_ranks([e2e], torch.distributed.ReduceOp.MAX, "cuda")[0]
         return {"ms": total / args.steps, "per_step": per_step, "e2e_ms": e2e, "e2e_wall_ms": wall,
                 "clocks": cs.summary(local), "launches": b.launches_per_run * args.steps}
 
@@ -511,10 +525,15 @@ def main():
     batch.close()
     torch.cuda.empty_cache()
     err = mixed_error(bt, mols, pds, ads, args.fp32_threshold, torch)
+    if world > 1:  # every rank's mixed result must pass for the mixed headline
+        err["max_abs"] = reduce_over_ranks([err["max_abs"]], torch.distributed.ReduceOp.MAX, "cuda")[0]
     mixed_ok = err["max_abs"] <= 1e-10
     head = mmix if mixed_ok else m64
 
-    screened = tot["screened"] * world
+    # whole-job units: the shards differ, so sum them over the ranks
+    screened, primitive, contracted, atoms = reduce_over_ranks(
+        [tot["screened"], tot["primitive"], tot["contracted"], sum(len(m.elements) for m in mols)],
+        torch.distributed.ReduceOp.SUM if world > 1 else None, "cuda")
     value = screened / (head["ms"] * 1e-3)
     dom = max(class_ms, key=class_ms.get) if class_ms else None
     roof = None
@@ -542,7 +561,7 @@ def main():
                    "sample": f"molecules {smp['molecules']} of the batch (dense output <= 2e8 doubles each), "
                              f"{smp['triplets']} screened triplets, {smp['seconds']:.1f} s"}
             dropin = dropin_sample(mols, pds, ads, stats, smp["molecules"])
-    serving = run_serving(args, torch, args.seed + 1000 * rank) if args.serve_requests > 0 else None
+    serving = run_serving(args, torch, args.seed) if args.serve_requests > 0 and rank == 0 else None
     config2 = run_config2(torch, bt, args.fp32_threshold, args.seed) if not args.no_config2 and rank == 0 else None
     if rank == 0:
         per = head["per_step"]
@@ -552,11 +571,11 @@ def main():
             "vs_baseline": None, "dtype": "f64+f32 (mixed)" if mixed_ok else "f64",
             "data": "synthetic (seeded generators; no dataset)",
             "config": {"workload": WORKLOAD, "molecules": args.molecules * world, "seed": args.seed,
-                       "atoms": sum(len(m.elements) for m in mols) * world,
+                       "atoms": int(atoms),
                        "precision": "mixed" if mixed_ok else "fp64",
-                       "classes": len(per_class), "primitive_triplets_per_step": tot["primitive"] * world,
-                       "contracted_triplets_per_step": tot["contracted"] * world,
-                       "screened_triplets_per_step": screened, "threshold": THRESHOLD,
+                       "classes": len(per_class), "primitive_triplets_per_step": int(primitive),
+                       "contracted_triplets_per_step": int(contracted),
+                       "screened_triplets_per_step": int(screened), "threshold": THRESHOLD,
                        "packed_output_bytes": out_bytes, "input_table_bytes": table_bytes,
                        "l2": "inputs + packed output per step exceed the 126 MB L2 (no flush needed)",
                        "parallelism": f"{world} independent shard(s)"},
