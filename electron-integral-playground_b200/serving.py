@@ -19,10 +19,11 @@ asking for S, V, (P|Q) and (mu nu|P).  The server
   window alone on its request's resident batch; up to `max_inflight` launches
   overlap on the device;
 * when a launch completes, hands each of its pieces' packed class blocks
-  (device views into the arena) to `consumer(request, piece, blocks)` (default:
-  a per-request digest, sum of squares, on the device) and frees the launch's
-  arena range; S comes from the drop-in overlap entry point on a worker thread
-  while the GPU works.
+  (device views into the arena) to `consumer(request, piece, blocks)` on a
+  consumer stream (default: a per-request digest, sum of squares, on the
+  device), and frees the launch's arena range once the consumer's work has
+  finished — the loop never waits for it; S comes from the drop-in overlap
+  entry point on a worker thread while the GPU works.
 
 Latency of a request = completion of its last piece minus its arrival.
 Precision "mixed" uses the batch's FP32 gate for (mu nu|P) (<= 1e-10 of FP64,
@@ -120,6 +121,7 @@ class Request:
         self.arrival = arrival
         self.pieces_left = 0
         self.digest = 0.0
+        self.digest_dev = None  # device accumulator of the default consumer
         self.done = None
         self.S = None
         self.resident = None  # the resident batch of a windowed request (or its pending build)
@@ -193,9 +195,11 @@ class Arena:
 
 def default_consumer(request, piece, blocks):
     """blocks: [((l_i, l_j, l_k), device view of the packed block)] of one piece;
-    adds the sum of squares of every value (one read of each block)."""
+    adds the sum of squares of every value (one read of each block) to the
+    request's device-side digest, without waiting for it."""
     if blocks:
-        request.digest += float(sum(v.dot(v) for _, v in blocks))
+        part = sum(v.dot(v) for _, v in blocks)
+        request.digest_dev = part if request.digest_dev is None else request.digest_dev + part
 
 
 class IntegralServer:
@@ -217,6 +221,9 @@ class IntegralServer:
         # finished batches: destroyed only while nothing is in flight, because
         # freeing device memory synchronises the whole device
         self._dead = []
+        # launches whose consumer work is queued: (event, off, alloc, pieces)
+        self._consuming = []
+        self.cstream = torch.cuda.Stream()
         # host seconds spent planning pieces, building batches, retiring launches
         self.host_s = {"plan": 0.0, "build": 0.0, "retire": 0.0}
 
@@ -283,9 +290,13 @@ class IntegralServer:
         if self.host_overlap:
             worker.start()
         # resident batches of windowed requests are built on a builder thread
-        # as the requests arrive, overlapping the loop and the GPU
-        builder = concurrent.futures.ThreadPoolExecutor(max_workers=1)
+        # as the requests arrive; launches (a batch build + graph launch, or a
+        # window) run in admission order on a launcher thread; both overlap the
+        # loop and the GPU
         device = self.torch.cuda.current_device()
+        init = (lambda: self.torch.cuda.set_device(device))
+        builder = concurrent.futures.ThreadPoolExecutor(max_workers=1, initializer=init)
+        launcher = concurrent.futures.ThreadPoolExecutor(max_workers=1, initializer=init)
         t0 = time.perf_counter()
         finished = []
         n_total = len(todo)
@@ -305,16 +316,18 @@ class IntegralServer:
                     waiting.extend(ps)
                     if self.host_overlap:
                         hostq.put(req)
-                for item in list(inflight):
-                    if item[1].query():
+                for fut in list(inflight):
+                    if fut.done() and fut.result()[1].query():
                         tr = time.perf_counter()
-                        self._retire(item, finished, t0)
+                        self._retire(fut.result())
                         self.host_s["retire"] += time.perf_counter() - tr
-                        inflight.remove(item)
-                if self._dead and (not inflight or len(self._dead) > 64):
-                    for b in self._dead:
-                        b.close()
-                    self._dead.clear()
+                        inflight.remove(fut)
+                for entry in list(self._consuming):
+                    if entry[0].query():
+                        self._consumed(entry, finished, t0)
+                        self._consuming.remove(entry)
+                if self._dead and ((not inflight and not self._consuming) or len(self._dead) > 64):
+                    self._close_dead()
                 if waiting and len(inflight) < self.max_inflight:
                     largest = self.arena.largest_free
                     group, total = [], 0
@@ -330,27 +343,27 @@ class IntegralServer:
                             total += p.elems
                     if group:
                         off, alloc = self.arena.alloc(total + 32 * len(group))
-                        tb = time.perf_counter()
                         if group[0].window:
-                            inflight.append(self._launch_window(group[0], off, alloc))
+                            inflight.append(launcher.submit(self._launch_window, group[0], off, alloc))
                         else:
-                            inflight.append(self._launch(group, off, alloc))
-                        self.host_s["build"] += time.perf_counter() - tb
+                            inflight.append(launcher.submit(self._launch, group, off, alloc))
                         continue
-                    if not inflight:
+                    if not inflight and not self._consuming:
                         raise RuntimeError("a piece does not fit the empty arena")
                 if not inflight and not waiting and todo and realtime:
                     time.sleep(max(0.0, min(0.002, todo[0].arrival - (time.perf_counter() - t0))))
                 else:
                     time.sleep(0.0002)
         finally:
-            for item in inflight:
+            launcher.shutdown(wait=True)
+            items = [f.result() for f in inflight if f.exception() is None]
+            for item in items:
                 item[0].sync()
-            for item in inflight:
+            for item in items:
                 item[0].close()
-            for b in self._dead:
-                b.close()
-            self._dead.clear()
+            self.cstream.synchronize()
+            self._consuming.clear()
+            self._close_dead()
             builder.shutdown(wait=True)
             for r in requests:
                 if r.resident is not None:
@@ -369,8 +382,10 @@ class IntegralServer:
 
     def _launch(self, group, off, alloc):
         """One batch (one CUDA-graph launch) over every piece of the group, its
-        output bound to the group's arena range; returns the in-flight record."""
+        output bound to the group's arena range; returns the in-flight record.
+        Runs on the launcher thread."""
         torch = self.torch
+        tb = time.perf_counter()
         kw = {} if self.fp32_threshold is None else {"fp32_threshold": self.fp32_threshold}
         b = ThreeCenterBatch([p.request.molecule for p in group], [p.pair_data for p in group],
                              [p.aux_data for p in group], precision=self.precision,
@@ -384,12 +399,14 @@ class IntegralServer:
         ev.record(torch.cuda.ExternalStream(b.stream))
         self.launches += 1
         layout = [self._layout(p, lambda li, lj, lk, m=m: b.block(m, li, lj, lk)) for m, p in enumerate(group)]
+        self.host_s["build"] += time.perf_counter() - tb
         return (b, ev, group, off, alloc, layout)
 
     def _launch_window(self, piece, off, alloc):
         """One auxiliary window of a large request on its resident batch (built
-        and uploaded at the first window)."""
+        on the builder thread).  Runs on the launcher thread."""
         torch = self.torch
+        tb = time.perf_counter()
         req = piece.request
         if isinstance(req.resident, concurrent.futures.Future):
             req.resident = req.resident.result()
@@ -402,6 +419,7 @@ class IntegralServer:
         ev = torch.cuda.Event()
         ev.record(torch.cuda.ExternalStream(b.stream))
         self.launches += 1
+        self.host_s["build"] += time.perf_counter() - tb
         return (b, ev, [piece], off, alloc, layout)
 
     @staticmethod
@@ -416,38 +434,49 @@ class IntegralServer:
             out.append(((li, lj, lk), o, nsp * (2 * li + 1) * (2 * lj + 1) * (2 * max(lk, 0) + 1) * nax))
         return out
 
-    def _retire(self, item, finished, t0):
+    def _retire(self, item):
+        """A launch has completed: queue the consumer's work on the consumer
+        stream (the completion event has been seen, so the output is final; no
+        stream wait, since a windowed batch's stream may already hold its next
+        window) and remember when that work will have finished."""
         batch, _, pieces, off, alloc, layout = item
-        windowed = pieces[0].window
-        if not windowed:
-            batch.status()
-        # the launch's completion event has been seen, so the consumer's kernels
-        # (torch's current stream) read finished output; no stream wait (a
-        # windowed batch's stream may already hold its next window)
         torch = self.torch
-        for p, lay in zip(pieces, layout):
-            blocks = [(c, self.arena.buf[off + o:off + o + n]) for c, o, n in lay]
-            self.consumer(p.request, p, blocks)
-            if self.keep_blocks:
-                for c, v in blocks:
-                    self.kept[p.request.rid][(p.kind, p.aux_lo) + c] = v.cpu().numpy().copy()
-            p.request.pieces_left -= 1
-            if p.request.pieces_left == 0:
-                p.request.done = time.perf_counter() - t0
-                finished.append(p.request)
-        # the consumer's work is queued on torch's stream; the range is reused
-        # only after it, so make the next batches wait for it
-        ev = torch.cuda.Event()
-        ev.record(torch.cuda.current_stream())
-        ev.synchronize()
-        self.arena.release(off, alloc)
-        if windowed:
+        with torch.cuda.stream(self.cstream):
+            for p, lay in zip(pieces, layout):
+                blocks = [(c, self.arena.buf[off + o:off + o + n]) for c, o, n in lay]
+                self.consumer(p.request, p, blocks)
+                if self.keep_blocks:
+                    for c, v in blocks:
+                        self.kept[p.request.rid][(p.kind, p.aux_lo) + c] = v.cpu().numpy().copy()
+            ev = torch.cuda.Event()
+            ev.record(self.cstream)
+        self._consuming.append((ev, off, alloc, pieces))
+        if pieces[0].window:
             req = pieces[0].request
             req.windows_left -= 1
-            if req.windows_left == 0:  # its last window: check every window's self-checks, free the tables
-                batch.status()
+            if req.windows_left == 0:  # its last window: free the tables later
                 self._dead.append(batch)
                 req.resident = None
         else:
             batch.bind_output(0)
             self._dead.append(batch)
+
+    def _consumed(self, entry, finished, t0):
+        """The consumer's work on a launch's output has finished: free the arena
+        range; a request is done when its last piece is."""
+        _, off, alloc, pieces = entry
+        self.arena.release(off, alloc)
+        for p in pieces:
+            p.request.pieces_left -= 1
+            if p.request.pieces_left == 0:
+                p.request.done = time.perf_counter() - t0
+                if p.request.digest_dev is not None:
+                    p.request.digest = float(p.request.digest_dev)
+                finished.append(p.request)
+
+    def _close_dead(self):
+        """Check the self-check words of finished batches and destroy them."""
+        for b in self._dead:
+            b.status()
+            b.close()
+        self._dead.clear()
