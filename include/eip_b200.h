@@ -116,6 +116,27 @@ int eip_three_center_noalloc(const int i_L, const int j_L, const int k_L,
                              const int n_aux_primitive_k, double* J3c_matrix, const int n_ao, const int n_aux,
                              const bool spherical, const double omega, void* stream);
 
+/* ---- screened pair tables built on the device (no counterpart in the C ABI:
+ * replaces the reference front end's Python form_pair_data,
+ * electron_integral_playground/pair_utility.py:6-188) ----------------------
+ * Shells in basis order: angular momentum, atom, first AO, primitive count;
+ * their primitives' exponents and (normalised) coefficients concatenated;
+ * geometry (n_atom, 3) in Bohr.  Keeps the primitive pairs whose bound is
+ * >= threshold (the reference front end uses 1e-14), stably sorted by
+ * descending bound per (l_i, l_j) class, with the reference's bound
+ * construction.  Results are held by the returned object: eip_pairs_count
+ * gives a class's row count (0 if absent), eip_pairs_copy copies its rows
+ * into host arrays (P_p, A_a, B_b: 4 doubles a row). */
+typedef struct eip_pairs eip_pairs;
+eip_pairs* eip_pairs_build(int n_shell, const int* shell_l, const int* shell_atom, const int* shell_ao,
+                           const int* shell_nprim, const double* prim_exp, const double* prim_coef, int n_atom,
+                           const double* geometry, double threshold);
+const char* eip_pairs_error(eip_pairs* pairs);
+int eip_pairs_count(eip_pairs* pairs, int i_L, int j_L);
+int eip_pairs_copy(eip_pairs* pairs, int i_L, int j_L, double* P_p, double* A_a, double* B_b, double* coefficient,
+                   int* i_ao_start, int* j_ao_start, int* i_atom, int* j_atom, double* upper_bound);
+void eip_pairs_destroy(eip_pairs* pairs);
+
 /* FMA-throughput microbenchmark on the current device (fp64 != 0: double,
  * else float), best of 5 runs, in TFLOP/s: the denominators of the rooflines. */
 int eip_measure_fma_peak(int fp64, double* tflops);
