@@ -313,25 +313,37 @@ int eip_batch_build(eip_batch* b) {
                 const int n = (int)p.ia.size();
                 group_indices(p.ia.data(), p.ja.data(), n, order, gb, gi, gj);
                 const int prim0 = (int)H.P.size();
-                for (size_t g = 0; g + 1 < gb.size(); g++) {
-                    H.ao.push_back(make_int2(gi[g], gj[g]));
+                const int ng = (int)gb.size() - 1;
+                const size_t g0 = H.ao.size();
+                H.ao.resize(g0 + ng);
+                H.AB.resize(g0 + ng);
+                H.bound.resize(g0 + ng);
+                H.begin.resize(g0 + 1 + ng);
+                H.P.resize((size_t)prim0 + n);
+                H.PA.resize((size_t)prim0 + n);
+                const int li = pc.first.first, lj = pc.first.second;
+                // each group and each primitive is independent: fill in parallel
+#pragma omp parallel for schedule(dynamic, 256)
+                for (int g = 0; g < ng; g++) {
+                    H.ao[g0 + g] = make_int2(gi[g], gj[g]);
                     const int q = order[gb[g]];
-                    H.AB.push_back(make_double4(p.A[4 * q] - p.B[4 * q], p.A[4 * q + 1] - p.B[4 * q + 1],
-                                                p.A[4 * q + 2] - p.B[4 * q + 2], 0.0));
-                    H.begin.push_back(prim0 + gb[g + 1]);
+                    H.AB[g0 + g] = make_double4(p.A[4 * q] - p.B[4 * q], p.A[4 * q + 1] - p.B[4 * q + 1],
+                                                p.A[4 * q + 2] - p.B[4 * q + 2], 0.0);
+                    H.begin[g0 + 1 + g] = prim0 + gb[g + 1];
                     double qb = 0.0;
                     for (int k = gb[g]; k < gb[g + 1]; k++) {
                         const int r = order[k];
-                        qb += pair_bound(&p.A[4 * r], &p.B[4 * r], p.coef[r], pc.first.first, pc.first.second);
+                        qb += pair_bound(&p.A[4 * r], &p.B[4 * r], p.coef[r], li, lj);
                     }
-                    H.bound.push_back(qb);
+                    H.bound[g0 + g] = qb;
                 }
+#pragma omp parallel for schedule(static)
                 for (int k = 0; k < n; k++) {
                     const int q = order[k];
                     const double* P = &p.P[4 * q];
                     const double* A = &p.A[4 * q];
-                    H.P.push_back(make_double4(P[0], P[1], P[2], P[3]));
-                    H.PA.push_back(make_double4(P[0] - A[0], P[1] - A[1], P[2] - A[2], p.coef[q]));
+                    H.P[(size_t)prim0 + k] = make_double4(P[0], P[1], P[2], P[3]);
+                    H.PA[(size_t)prim0 + k] = make_double4(P[0] - A[0], P[1] - A[1], P[2] - A[2], p.coef[q]);
                 }
             }
             H.sp_begin.push_back((int)H.ao.size());

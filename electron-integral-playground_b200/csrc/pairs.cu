@@ -133,13 +133,28 @@ __global__ void pair_rows_kernel(int n_keep, const int* __restrict__ slot_of, in
     j_atom[r] = sj.atom;
 }
 
+// Stream-ordered device buffer: cudaMallocAsync / cudaFreeAsync on the build's
+// own stream, so building tables never synchronises the device (other
+// streams keep running kernels meanwhile).
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
+    cudaStream_t s = nullptr;
+    explicit DevBuf(cudaStream_t stream) : s(stream) {}
     ~DevBuf() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, s);
     }
-    cudaError_t alloc(size_t n) { return cudaMalloc((void**)&p, sizeof(T) * (n ? n : 1)); }
+    cudaError_t alloc(size_t n) { return cudaMallocAsync((void**)&p, sizeof(T) * (n ? n : 1), s); }
+};
+
+struct StreamHolder {
+    cudaStream_t s = nullptr;
+    ~StreamHolder() {
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    }
 };
 
 }  // namespace
@@ -176,22 +191,26 @@ eip_pairs* eip_pairs_build(int n_shell, const int* shell_l, const int* shell_ato
         snprintf(r->err, sizeof r->err, "device initialisation failed (%d)", rc);
         return r;
     }
+    StreamHolder sth;  // destroyed last: waits for the frees queued below
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&sth.s, cudaStreamNonBlocking)) != cudaSuccess)
+        return pairs_fail(r, "stream", e);
+    const cudaStream_t st = sth.s;
     std::vector<ShellRec> sh(n_shell);
     int n_prim = 0;
     for (int s = 0; s < n_shell; s++) {
         sh[s] = ShellRec{shell_l[s], shell_atom[s], shell_ao[s], shell_nprim[s], n_prim};
         n_prim += shell_nprim[s];
     }
-    DevBuf<ShellRec> d_sh;
-    DevBuf<double> d_exp, d_coef, d_geom;
-    cudaError_t e;
+    DevBuf<ShellRec> d_sh(st);
+    DevBuf<double> d_exp(st), d_coef(st), d_geom(st);
     if ((e = d_sh.alloc(n_shell)) || (e = d_exp.alloc(n_prim)) || (e = d_coef.alloc(n_prim)) ||
         (e = d_geom.alloc(3 * (size_t)n_atom)))
         return pairs_fail(r, "allocation", e);
-    cudaMemcpy(d_sh.p, sh.data(), sizeof(ShellRec) * n_shell, cudaMemcpyHostToDevice);
-    cudaMemcpy(d_exp.p, prim_exp, sizeof(double) * n_prim, cudaMemcpyHostToDevice);
-    cudaMemcpy(d_coef.p, prim_coef, sizeof(double) * n_prim, cudaMemcpyHostToDevice);
-    cudaMemcpy(d_geom.p, geometry, sizeof(double) * 3 * n_atom, cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(d_sh.p, sh.data(), sizeof(ShellRec) * n_shell, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_exp.p, prim_exp, sizeof(double) * n_prim, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_coef.p, prim_coef, sizeof(double) * n_prim, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_geom.p, geometry, sizeof(double) * 3 * n_atom, cudaMemcpyHostToDevice, st);
     // shell pairs of each class in the reference's loop order
     std::map<std::pair<int, int>, std::vector<PairRec>> by_class;
     std::map<std::pair<int, int>, int> slots;
@@ -205,43 +224,44 @@ eip_pairs* eip_pairs_build(int n_shell, const int* shell_l, const int* shell_ato
         }
     for (auto& kv : by_class) {
         const int np = (int)kv.second.size(), ns = slots[kv.first];
-        DevBuf<PairRec> d_pairs;
-        DevBuf<double> d_bound, d_key, d_key_sorted;
-        DevBuf<int> d_flag, d_pos, d_val, d_val_sorted;
+        DevBuf<PairRec> d_pairs(st);
+        DevBuf<double> d_bound(st), d_key(st), d_key_sorted(st);
+        DevBuf<int> d_flag(st), d_pos(st), d_val(st), d_val_sorted(st);
         if ((e = d_pairs.alloc(np)) || (e = d_bound.alloc(ns)) || (e = d_flag.alloc(ns)) || (e = d_pos.alloc(ns)) ||
             (e = d_key.alloc(ns)) || (e = d_val.alloc(ns)) || (e = d_key_sorted.alloc(ns)) ||
             (e = d_val_sorted.alloc(ns)))
             return pairs_fail(r, "allocation", e);
-        cudaMemcpy(d_pairs.p, kv.second.data(), sizeof(PairRec) * np, cudaMemcpyHostToDevice);
-        pair_bound_kernel<<<(np + 127) / 128, 128>>>(np, d_pairs.p, d_sh.p, d_exp.p, d_coef.p, d_geom.p, threshold,
-                                                     d_bound.p);
-        flag_kernel<<<(ns + 255) / 256, 256>>>(ns, d_bound.p, d_flag.p);
+        cudaMemcpyAsync(d_pairs.p, kv.second.data(), sizeof(PairRec) * np, cudaMemcpyHostToDevice, st);
+        pair_bound_kernel<<<(np + 127) / 128, 128, 0, st>>>(np, d_pairs.p, d_sh.p, d_exp.p, d_coef.p, d_geom.p,
+                                                            threshold, d_bound.p);
+        flag_kernel<<<(ns + 255) / 256, 256, 0, st>>>(ns, d_bound.p, d_flag.p);
         size_t tmp_bytes = 0, tmp2 = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_flag.p, d_pos.p, ns);
         cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp2, d_key.p, d_key_sorted.p, d_val.p, d_val_sorted.p,
                                                   ns);
-        DevBuf<unsigned char> d_tmp;
+        DevBuf<unsigned char> d_tmp(st);
         if ((e = d_tmp.alloc(tmp_bytes > tmp2 ? tmp_bytes : tmp2))) return pairs_fail(r, "allocation", e);
-        cub::DeviceScan::ExclusiveSum(d_tmp.p, tmp_bytes, d_flag.p, d_pos.p, ns);
-        int last_pos = 0, last_flag = 0;
-        cudaMemcpy(&last_pos, d_pos.p + ns - 1, sizeof(int), cudaMemcpyDeviceToHost);
-        cudaMemcpy(&last_flag, d_flag.p + ns - 1, sizeof(int), cudaMemcpyDeviceToHost);
-        const int n_keep = last_pos + last_flag;
+        cub::DeviceScan::ExclusiveSum(d_tmp.p, tmp_bytes, d_flag.p, d_pos.p, ns, st);
+        int last[2] = {0, 0};
+        cudaMemcpyAsync(&last[0], d_pos.p + ns - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&last[1], d_flag.p + ns - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return pairs_fail(r, "bounds", e);
+        const int n_keep = last[0] + last[1];
         if (n_keep == 0) continue;
-        compact_kernel<<<(ns + 255) / 256, 256>>>(ns, d_bound.p, d_flag.p, d_pos.p, d_key.p, d_val.p);
+        compact_kernel<<<(ns + 255) / 256, 256, 0, st>>>(ns, d_bound.p, d_flag.p, d_pos.p, d_key.p, d_val.p);
         // stable: equal bounds keep the insertion (loop) order
         size_t tmp_sort = tmp2;
         cub::DeviceRadixSort::SortPairsDescending(d_tmp.p, tmp_sort, d_key.p, d_key_sorted.p, d_val.p,
-                                                  d_val_sorted.p, n_keep);
-        DevBuf<double> P, A, B, coef;
-        DevBuf<int> iao, jao, iat, jat;
+                                                  d_val_sorted.p, n_keep, 0, sizeof(double) * 8, st);
+        DevBuf<double> P(st), A(st), B(st), coef(st);
+        DevBuf<int> iao(st), jao(st), iat(st), jat(st);
         if ((e = P.alloc(4 * (size_t)n_keep)) || (e = A.alloc(4 * (size_t)n_keep)) ||
             (e = B.alloc(4 * (size_t)n_keep)) || (e = coef.alloc(n_keep)) || (e = iao.alloc(n_keep)) ||
             (e = jao.alloc(n_keep)) || (e = iat.alloc(n_keep)) || (e = jat.alloc(n_keep)))
             return pairs_fail(r, "allocation", e);
-        pair_rows_kernel<<<(n_keep + 127) / 128, 128>>>(n_keep, d_val_sorted.p, np, d_pairs.p, d_sh.p, d_exp.p,
-                                                        d_coef.p, d_geom.p, P.p, A.p, B.p, coef.p, iao.p, jao.p,
-                                                        iat.p, jat.p);
+        pair_rows_kernel<<<(n_keep + 127) / 128, 128, 0, st>>>(n_keep, d_val_sorted.p, np, d_pairs.p, d_sh.p,
+                                                               d_exp.p, d_coef.p, d_geom.p, P.p, A.p, B.p, coef.p,
+                                                               iao.p, jao.p, iat.p, jat.p);
         if ((e = cudaGetLastError()) != cudaSuccess) return pairs_fail(r, "kernels", e);
         eip_pairs::Class& c = r->classes[kv.first];
         c.n = n_keep;
@@ -254,15 +274,16 @@ eip_pairs* eip_pairs_build(int n_shell, const int* shell_l, const int* shell_ato
         c.j_ao.resize(n_keep);
         c.i_atom.resize(n_keep);
         c.j_atom.resize(n_keep);
-        cudaMemcpy(c.P.data(), P.p, sizeof(double) * 4 * n_keep, cudaMemcpyDeviceToHost);
-        cudaMemcpy(c.A.data(), A.p, sizeof(double) * 4 * n_keep, cudaMemcpyDeviceToHost);
-        cudaMemcpy(c.B.data(), B.p, sizeof(double) * 4 * n_keep, cudaMemcpyDeviceToHost);
-        cudaMemcpy(c.coef.data(), coef.p, sizeof(double) * n_keep, cudaMemcpyDeviceToHost);
-        cudaMemcpy(c.bound.data(), d_key_sorted.p, sizeof(double) * n_keep, cudaMemcpyDeviceToHost);
-        cudaMemcpy(c.i_ao.data(), iao.p, sizeof(int) * n_keep, cudaMemcpyDeviceToHost);
-        cudaMemcpy(c.j_ao.data(), jao.p, sizeof(int) * n_keep, cudaMemcpyDeviceToHost);
-        cudaMemcpy(c.i_atom.data(), iat.p, sizeof(int) * n_keep, cudaMemcpyDeviceToHost);
-        if ((e = cudaMemcpy(c.j_atom.data(), jat.p, sizeof(int) * n_keep, cudaMemcpyDeviceToHost)) != cudaSuccess)
+        cudaMemcpyAsync(c.P.data(), P.p, sizeof(double) * 4 * n_keep, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(c.A.data(), A.p, sizeof(double) * 4 * n_keep, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(c.B.data(), B.p, sizeof(double) * 4 * n_keep, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(c.coef.data(), coef.p, sizeof(double) * n_keep, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(c.bound.data(), d_key_sorted.p, sizeof(double) * n_keep, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(c.i_ao.data(), iao.p, sizeof(int) * n_keep, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(c.j_ao.data(), jao.p, sizeof(int) * n_keep, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(c.i_atom.data(), iat.p, sizeof(int) * n_keep, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(c.j_atom.data(), jat.p, sizeof(int) * n_keep, cudaMemcpyDeviceToHost, st);
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
             return pairs_fail(r, "copy", e);
     }
     return r;

@@ -40,9 +40,6 @@ import numpy as np
 
 from .batch import POINT_CHARGES, ThreeCenterBatch, metric_pair_tables
 
-_Z = {"H": 1.0, "He": 2.0, "C": 6.0, "N": 7.0, "O": 8.0, "F": 9.0}
-
-
 def aux_slices(aux_data, n_aux, max_functions):
     """Split the auxiliary tables into slices of whole shells, at most
     max_functions functions each (one shell at least), starts rebased to the
@@ -113,7 +110,11 @@ def window_elems(pair_sp, aux_starts, lo, hi):
 
 
 class Request:
-    def __init__(self, rid, molecule, pair_data, aux_data, arrival=0.0):
+    """One molecule's integrals.  pair_data / aux_data: the C-ABI tables, or
+    None to have the server build them (pair tables on the device) when the
+    request arrives."""
+
+    def __init__(self, rid, molecule, pair_data=None, aux_data=None, arrival=0.0):
         self.rid = rid
         self.molecule = molecule
         self.pair_data = pair_data
@@ -127,7 +128,7 @@ class Request:
         self.resident = None  # the resident batch of a windowed request (or its pending build)
         self.windows_left = 0
         self.charges = None
-
+        self.tables = None  # pending table build
 
 class Piece:
     """One molecule slot of a batch: kind "3c" ((mu nu|P) of the auxiliary
@@ -261,6 +262,16 @@ class IntegralServer:
                 raise ValueError(f"request {req.rid}: one auxiliary shell slice exceeds the HBM budget")
         return out
 
+    @staticmethod
+    def _build_tables(req):
+        """Pair tables on the device, auxiliary tables on the host (builder thread)."""
+        from .device_pairs import form_pair_data_device
+        from .pair_utility import form_auxiliary_pair_data
+
+        req.pair_data = form_pair_data_device(req.molecule, 1e-14)
+        req.aux_data = form_auxiliary_pair_data(req.molecule)
+        return req
+
     def _build_resident(self, req, device):
         """Resident batch of a windowed request (runs on the builder thread)."""
         self.torch.cuda.set_device(device)
@@ -283,6 +294,8 @@ class IntegralServer:
         """Serve `requests` (each with .arrival seconds from start); returns stats.
         realtime=False admits every request at once (arrival ignored)."""
         todo = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        preparing = []  # arrived, tables being built
+        arrived = collections.deque()  # arrived with tables, not yet split
         waiting = collections.deque()  # pieces of arrived requests, FIFO
         inflight = []
         hostq = queue.Queue()
@@ -295,7 +308,7 @@ class IntegralServer:
         # loop and the GPU
         device = self.torch.cuda.current_device()
         init = (lambda: self.torch.cuda.set_device(device))
-        builder = concurrent.futures.ThreadPoolExecutor(max_workers=1, initializer=init)
+        builder = concurrent.futures.ThreadPoolExecutor(max_workers=2, initializer=init)
         launcher = concurrent.futures.ThreadPoolExecutor(max_workers=1, initializer=init)
         t0 = time.perf_counter()
         finished = []
@@ -307,6 +320,17 @@ class IntegralServer:
                     req = todo.popleft()
                     if not realtime:
                         req.arrival = now
+                    if req.pair_data is None or req.aux_data is None:
+                        req.tables = builder.submit(self._build_tables, req)
+                        preparing.append(req)
+                    else:
+                        arrived.append(req)
+                for req in [r for r in preparing if r.tables.done()]:
+                    preparing.remove(req)
+                    req.tables.result()  # re-raises a failed build
+                    arrived.append(req)
+                while arrived:
+                    req = arrived.popleft()
                     tp = time.perf_counter()
                     ps = self.pieces_of(req)
                     self.host_s["plan"] += time.perf_counter() - tp
@@ -350,7 +374,7 @@ class IntegralServer:
                         continue
                     if not inflight and not self._consuming:
                         raise RuntimeError("a piece does not fit the empty arena")
-                if not inflight and not waiting and todo and realtime:
+                if not inflight and not waiting and not preparing and todo and realtime:
                     time.sleep(max(0.0, min(0.002, todo[0].arrival - (time.perf_counter() - t0))))
                 else:
                     time.sleep(0.0002)

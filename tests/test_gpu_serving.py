@@ -92,3 +92,21 @@ def test_served_blocks_match_drop_in(budget):
                                        atol=max(1e-12, 1e-13 * float(np.abs(ref).max())))
         n_cols += nax * nQ
     assert n_cols == M.shape[0] * len(r.aux_data)  # every column once per l_P
+
+
+def test_server_builds_tables_when_requests_carry_molecules_only():
+    """Requests without tables: the server builds them (pair tables on the
+    device) after arrival; the results equal those from the front end's tables
+    to rounding (the device tables differ from numpy's in the last bits)."""
+    reqs = _requests([4, 9])
+    a = sv.IntegralServer(budget_bytes=48e6, precision="fp64", keep_blocks=True, host_overlap=False)
+    a.serve([_fresh(r) for r in reqs], realtime=False)
+    b = sv.IntegralServer(budget_bytes=48e6, precision="fp64", keep_blocks=True, host_overlap=False)
+    bare = [sv.Request(r.rid, r.molecule, arrival=r.arrival) for r in reqs]
+    b.serve(bare, realtime=True)
+    for r in reqs:
+        ka, kb = a.kept[r.rid], b.kept[r.rid]
+        assert ka.keys() == kb.keys()
+        for k in ka:
+            scale = max(1.0, float(np.max(np.abs(ka[k]))) if ka[k].size else 1.0)
+            assert float(np.max(np.abs(ka[k] - kb[k]), initial=0.0)) <= 1e-12 * scale, (r.rid, k)
