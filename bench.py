@@ -521,6 +521,25 @@ def main():
         torch.cuda.synchronize()
         class_ms[(li, lj, lk)] = ev0.elapsed_time(ev1) / 2
     batch.status()
+    # The dominant class's FP32 kernel (the mixed path's FP32 half) alone: a
+    # batch whose every shell pair takes FP32, bound to the same output.
+    dom = max(class_ms, key=class_ms.get) if class_ms else None
+    fp32_dom_ms = None
+    if dom:
+        all32 = bt.ThreeCenterBatch(mols, pds, ads, precision="mixed", fp32_threshold=float("inf"))
+        all32.bind_output(out_ptr)
+        s32 = torch.cuda.ExternalStream(all32.stream)
+        if all32.run_class(*dom):
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(s32)
+            for _ in range(2):
+                all32.run_class(*dom)
+            ev1.record(s32)
+            torch.cuda.synchronize()
+            fp32_dom_ms = ev0.elapsed_time(ev1) / 2
+        all32.status()
+        all32.bind_output(0)
+        all32.close()
     fp64_peak = bt.measure_fma_peak(True)
     fp32_peak = bt.measure_fma_peak(False)
     batch.close()
@@ -532,11 +551,10 @@ def main():
     head = mmix if mixed_ok else m64
 
     # whole-job units: the shards differ, so sum them over the ranks
-    screened, primitive, contracted, atoms = reduce_over_ranks(
-        [tot["screened"], tot["primitive"], tot["contracted"], sum(len(m.elements) for m in mols)],
+    screened, primitive, contracted, atoms, out_elems_total = reduce_over_ranks(
+        [tot["screened"], tot["primitive"], tot["contracted"], sum(len(m.elements) for m in mols), out_bytes / 8],
         torch.distributed.ReduceOp.SUM if world > 1 else None, "cuda")
     value = screened / (head["ms"] * 1e-3)
-    dom = max(class_ms, key=class_ms.get) if class_ms else None
     roof = None
     if dom:
         achieved = per_class[dom]["flops"] / (class_ms[dom] * 1e-3) / 1e12
@@ -552,7 +570,13 @@ def main():
                 "algorithmic_flops_per_launch": per_class[dom]["flops"], "ms_per_launch": class_ms[dom],
                 "whole_step_tflops_fp64": tot["flops"] / (m64["ms"] * 1e-3) / 1e12,
                 "whole_step_frac_fp64": tot["flops"] / (m64["ms"] * 1e-3) / 1e12 / fp64_peak,
-                "output_store_gbs": tot["out_bytes"] / (head["ms"] * 1e-3) / 1e9}
+                "output_store_gbs": tot["out_bytes"] / (head["ms"] * 1e-3) / 1e9,
+                "fp32_kernel": None if fp32_dom_ms is None else {
+                    "kernel": f"k3c_fast<{dom[0]},{dom[1]},{dom[2]}> (FP32, every shell pair)",
+                    "ms_per_launch": fp32_dom_ms,
+                    "achieved": per_class[dom]["flops"] / (fp32_dom_ms * 1e-3) / 1e12, "peak": fp32_peak,
+                    "frac": per_class[dom]["flops"] / (fp32_dom_ms * 1e-3) / 1e12 / fp32_peak,
+                    "peak_source": "FP32 FMA microbenchmark on this GPU, this run"}}
     cpu = None
     dropin = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -586,6 +610,8 @@ def main():
                           "fp32_fraction_of_triplets": split32 / max(1, split32 + split64),
                           "mixed_vs_fp64_error": err, "fp32_fma_peak_tflops": fp32_peak,
                           "headline": "mixed" if mixed_ok else "fp64"},
+            "integrals_per_s": {"value": out_elems_total / (head["ms"] * 1e-3),
+                                "what": "spherical (mu nu|P) values written per second (packed, i<=j shell pairs)"},
             "e2e": {"value": screened / (head["e2e_ms"] * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": table_bytes["mixed" if mixed_ok else "fp64"],
                     "d2h_bytes_per_step": 8 * len(mols),
