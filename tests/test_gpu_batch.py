@@ -247,3 +247,21 @@ def test_window_runs_reproduce_the_full_run(small_batch):
                         seen += want.size
             assert seen == n
         b.close()
+
+
+def test_cartesian_batch_matches_drop_in():
+    """Cartesian output (every class on the generic kernels inside the graph)."""
+    mols = []
+    for i, n in enumerate([3, 4]):
+        m = syn.organic_molecule(n, seed=300 + i)
+        syn.attach_synthetic_basis(m, aux_l_max=3, seed=1, spherical=False)
+        mols.append(m)
+    pds = [pu.form_pair_data(m, 1e-14) for m in mols]
+    ads = [pu.form_auxiliary_pair_data(m) for m in mols]
+    b = bt.ThreeCenterBatch(mols, pds, ads)
+    b.alloc_output()
+    b.run()
+    b.status()
+    for m in range(len(mols)):
+        np.testing.assert_allclose(b.dense(m), mi.three_center(pds[m], ads[m], mols[m]), rtol=0, atol=1e-13)
+    b.close()
