@@ -120,6 +120,7 @@ def main():
     for kind, name, status, rec in cases:
         save_case(kind, name, status, rec)
     save_pair_counts(args.reference)
+    save_normalisation(args.reference)
 
 
 def pack_pairs(prefix, table, out):
@@ -204,6 +205,38 @@ def save_pair_counts(reference):
         pack_pairs("pair__", form_pair_data(mol, 1e-14), out)
         np.savez_compressed(HERE / f"{name}.npz", **out)
         print("pair counts", name)
+
+
+def save_normalisation(reference):
+    """normalize_shell on every shell of the bundled orbital and auxiliary
+    basis sets for H, C, N, O, F (the reference's own basis library)."""
+    from copy import deepcopy
+
+    from electron_integral_playground.basis_reader.gaussian_basis_reader import read_basis
+    from electron_integral_playground.basis_utility import normalize_shell
+
+    out = {}
+    k = 0
+    data = pathlib.Path(reference) / "electron_integral_playground" / "data" / "basis_sets"
+    names = sorted(p.name.split(".")[0] for p in data.iterdir() if p.name.endswith(".basis"))
+    for basis_name in names:
+        try:
+            basis = read_basis(basis_name)
+        except Exception as exc:  # a basis the reference does not bundle
+            print("skip", basis_name, exc)
+            continue
+        for el in ("H", "C", "N", "O", "F"):
+            for s in basis.get(el, []):
+                t = deepcopy(s)
+                normalize_shell(t)
+                out[f"l_{k}"] = np.array(int(s.angular))
+                out[f"exp_{k}"] = np.array(s.primitive_exponents, dtype=np.float64)
+                out[f"raw_{k}"] = np.array(s.primitive_coefficients, dtype=np.float64)
+                out[f"norm_{k}"] = np.array(t.primitive_coefficients, dtype=np.float64)
+                k += 1
+    out["n"] = np.array(k)
+    np.savez_compressed(HERE / "normalize_shell.npz", **out)
+    print("normalize_shell shells", k)
 
 
 if __name__ == "__main__":

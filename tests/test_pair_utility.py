@@ -73,3 +73,24 @@ def test_synthetic_generators_terminate_and_respect_geometry():
     o = w.geometry[0::3] * 0.52917721054482
     d = np.linalg.norm(o[:, None] - o[None], axis=-1)
     assert np.min(d[np.triu_indices(10, 1)]) >= 2.6
+
+
+def test_normalize_shell_matches_reference_on_bundled_bases():
+    """normalize_shell against the reference's on every H/C/N/O/F shell of the
+    reference's bundled orbital and auxiliary basis sets (fixture made by
+    tests/golden/make_golden.py): bit for bit."""
+    import pathlib
+    from copy import deepcopy
+
+    bu = importlib.import_module("electron-integral-playground_b200.basis_utility")
+    ds = importlib.import_module("electron-integral-playground_b200.data_structure")
+    f = np.load(pathlib.Path(__file__).parent / "golden" / "normalize_shell.npz")
+    n = int(f["n"])
+    assert n > 100
+    for k in range(n):
+        s = ds.GaussianShell(angular=int(f[f"l_{k}"]), i_ao_start=-1, i_atom=-1,
+                             primitive_exponents=f[f"exp_{k}"].copy(), primitive_coefficients=f[f"raw_{k}"].copy())
+        t = deepcopy(s)
+        bu.normalize_shell(t)
+        np.testing.assert_array_equal(t.primitive_exponents, f[f"exp_{k}"])
+        np.testing.assert_array_equal(t.primitive_coefficients, f[f"norm_{k}"], err_msg=f"shell {k}")
