@@ -555,6 +555,11 @@ def main():
         [tot["screened"], tot["primitive"], tot["contracted"], sum(len(m.elements) for m in mols), out_bytes / 8],
         torch.distributed.ReduceOp.SUM if world > 1 else None, "cuda")
     value = screened / (head["ms"] * 1e-3)
+    hbm_peak = None
+    try:
+        hbm_peak = float(json.loads((REPO / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+    except Exception:
+        pass
     roof = None
     if dom:
         achieved = per_class[dom]["flops"] / (class_ms[dom] * 1e-3) / 1e12
@@ -571,6 +576,9 @@ def main():
                 "whole_step_tflops_fp64": tot["flops"] / (m64["ms"] * 1e-3) / 1e12,
                 "whole_step_frac_fp64": tot["flops"] / (m64["ms"] * 1e-3) / 1e12 / fp64_peak,
                 "output_store_gbs": tot["out_bytes"] / (head["ms"] * 1e-3) / 1e9,
+                "hbm_peak_gbs": hbm_peak, "output_store_frac_of_hbm": (
+                    None if hbm_peak is None else tot["out_bytes"] / (head["ms"] * 1e-3) / 1e9 / hbm_peak),
+                "hbm_peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth measured on this pool)",
                 "fp32_kernel": None if fp32_dom_ms is None else {
                     "kernel": f"k3c_fast<{dom[0]},{dom[1]},{dom[2]}> (FP32, every shell pair)",
                     "ms_per_launch": fp32_dom_ms,
