@@ -62,6 +62,7 @@ def _bind(L):
     L.eip_batch_add_charges.argtypes = [_vp, c_int, _dpp, c_int]
     L.eip_batch_build.argtypes = [_vp]
     L.eip_batch_set_precision.argtypes = [_vp, c_int, c_double]
+    L.eip_batch_set_streams.argtypes = [_vp, c_int]
     L.eip_batch_precision_split.argtypes = [_vp, c_int, c_int, c_int, ctypes.POINTER(c_ll), ctypes.POINTER(c_ll)]
     L.eip_batch_output_elems.argtypes = [_vp]
     L.eip_batch_output_elems.restype = c_ll
@@ -166,6 +167,10 @@ class ThreeCenterBatch:
 
     def bind_output(self, device_ptr: int):
         self._check(self.L.eip_batch_bind_output(self.h, ctypes.c_void_p(device_ptr)), "bind_output")
+
+    def set_streams(self, n: int):
+        """Streams the class kernels are forked over (before the first run)."""
+        self._check(self.L.eip_batch_set_streams(self.h, int(n)), "set_streams")
 
     def run(self, checksum: bool = False, sync: bool = True):
         self._check(self.L.eip_batch_run(self.h, 1 if checksum else 0), "run")

@@ -95,6 +95,7 @@ struct eip_batch {
     bool spherical = true;
     double omega = 0.0;
     int precision = 0;     // 0 FP64, 1 mixed (FP32 for bounded shell pairs)
+    int n_streams = 4;     // streams the class kernels are forked over
     double fp32_tau = 0.0;
     std::vector<std::map<std::pair<int, int>, PairIn>> pairs;  // per molecule
     std::vector<std::map<int, AuxIn>> aux;                     // per molecule
@@ -214,6 +215,12 @@ double transform_gain(int l, bool spherical) {
 }  // namespace
 
 extern "C" {
+
+int eip_batch_set_streams(eip_batch* b, int n_streams) {
+    if (!b || b->exec || !b->side.empty() || n_streams < 1 || n_streams > 8) return 2;
+    b->n_streams = n_streams;
+    return 0;
+}
 
 int eip_batch_set_precision(eip_batch* b, int mode, double fp32_threshold) {
     if (!b || b->built || mode < 0 || mode > 1 || !(fp32_threshold >= 0.0)) return 2;
@@ -623,7 +630,7 @@ double* eip_batch_output_device(eip_batch* b) { return b ? b->d_out : nullptr; }
 
 static int capture(eip_batch* b, bool checksum) {
     cudaError_t e;
-    const int n_side = 4;
+    const int n_side = b->n_streams;
     if (b->side.empty()) {
         for (int i = 0; i < n_side; i++) {
             cudaStream_t s;
@@ -824,7 +831,7 @@ int eip_batch_run_window(eip_batch* b, double* device_out, int checksum) {
     if (!b || !b->built || !b->win_planned || !device_out) return 2;
     cudaError_t e;
     const int nm = b->n_mol;
-    const int n_side = 4;
+    const int n_side = b->n_streams;
     if (b->side.empty()) {
         for (int i = 0; i < n_side; i++) {
             cudaStream_t s;
