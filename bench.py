@@ -47,7 +47,7 @@ sys.path.insert(0, str(REPO))
 
 METRIC = "screened (μν|P) triplets/s, mixed vs FP64 at ≤1e-10 abs; p50/p99 latency"
 UNIT = "triplets/s"
-WORKLOAD = ("config-1 batched uneven sizes: 64 organic molecules of 3-60 atoms (log-uniform, H/C/N/O), "
+WORKLOAD = ("batched uneven sizes: 64 organic molecules of 3-60 atoms (log-uniform, H/C/N/O), "
             "orbital 3s2p1d/2s1p contracted, auxiliary s-g uncontracted, all (mu nu|P) spherical, "
             "one CUDA-graph launch")
 THRESHOLD = 1e-14
@@ -80,7 +80,7 @@ def build_workload(seed, n_mol):
     syn = importlib.import_module("electron-integral-playground_b200.synthetic")
     pu = importlib.import_module("electron-integral-playground_b200.pair_utility")
     rf = importlib.import_module("electron-integral-playground_b200.roofline")
-    mols = syn.config1_batch(seed, n_mol)
+    mols = syn.organic_batch(seed, n_mol)
     pds = [pu.form_pair_data(m, 1e-14) for m in mols]
     ads = [pu.form_auxiliary_pair_data(m) for m in mols]
     stats = [rf.class_statistics(pd, ad, THRESHOLD) for pd, ad in zip(pds, ads)]
@@ -273,7 +273,7 @@ def run_config2(torch, bt, threshold, seed=0, window_bytes=24e9):
     pu = importlib.import_module("electron-integral-playground_b200.pair_utility")
     rf = importlib.import_module("electron-integral-playground_b200.roofline")
     sv = importlib.import_module("electron-integral-playground_b200.serving")
-    mol = syn.config2_water100(seed)
+    mol = syn.water100_cluster(seed)
     pd, ad = pu.form_pair_data(mol, 1e-14), pu.form_auxiliary_pair_data(mol)
     stats = rf.class_statistics(pd, ad, 1e-12)
     screened = sum(v["screened"] for v in stats.values())
@@ -493,9 +493,10 @@ def main():
         return {"ms": total / args.steps, "per_step": per_step, "e2e_ms": e2e, "e2e_wall_ms": wall,
                 "clocks": cs.summary(local), "launches": b.launches_per_run * args.steps}
 
-    gdir = REPO / "gpurun_out"
-    cpath = (lambda tag: str(gdir / f"clocks_{tag}_rank{rank}.csv")) if gdir.is_dir() else \
-        (lambda tag: f"/tmp/eip_clocks_{tag}_{os.getpid()}.csv")
+    import tempfile
+
+    cdir = os.environ.get("EIP_BENCH_CLOCKS_DIR") or tempfile.gettempdir()
+    cpath = lambda tag: os.path.join(cdir, f"eip_clocks_{tag}_rank{rank}_{os.getpid()}.csv")
     m64 = measure(batch, cpath("fp64"))
     mmix = measure(mixed, cpath("mixed"))
     split64 = split32 = 0

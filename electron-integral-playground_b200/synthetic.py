@@ -190,12 +190,12 @@ def attach_synthetic_basis(molecule: Molecule, aux_l_max: int, seed: int = 0, sp
     return molecule
 
 
-def config0_water10(seed: int = 0) -> Molecule:
+def water10_cluster(seed: int = 0) -> Molecule:
     """10 waters in a 9 A cube; aux s-f."""
     return attach_synthetic_basis(water_cluster(10, 9.0, seed), aux_l_max=3, seed=seed)
 
 
-def config2_water100(seed: int = 0) -> Molecule:
+def water100_cluster(seed: int = 0) -> Molecule:
     """100 waters in a 15 A cube; aux s-f."""
     return attach_synthetic_basis(water_cluster(100, 15.0, seed), aux_l_max=3, seed=seed)
 
@@ -205,7 +205,7 @@ def molecule_sizes(n_molecule: int, lo: int, hi: int, seed: int):
     return [int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))))) for _ in range(n_molecule)]
 
 
-def config1_batch(seed: int = 0, n_molecule: int = 64):
+def organic_batch(seed: int = 0, n_molecule: int = 64):
     """64 organic molecules of 3-60 atoms (log-uniform); aux s-g."""
     sizes = molecule_sizes(n_molecule, 3, 60, seed)
     return [attach_synthetic_basis(organic_molecule(n, seed * 1000 + i), aux_l_max=4, seed=seed)
@@ -244,7 +244,7 @@ def random_shell_triplet(rng, l_orbital_max=4, l_aux_max=5, max_primitives=8, bo
     return (li, lj), pair, lk, aux, mol
 
 
-def config3_triplets(seed: int = 0, n: int = 2000):
+def random_shell_triplets(seed: int = 0, n: int = 2000):
     """2000 random shell triplets: centres in a 6 A cube, orbital l <= 4,
     auxiliary l <= 5, 1-8 primitives, exponents log-uniform in [0.05, 1e4]."""
     rng = np.random.default_rng(seed + 3)

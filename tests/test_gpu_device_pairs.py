@@ -18,7 +18,7 @@ mi = importlib.import_module("electron-integral-playground_b200.molecular_integr
 
 
 def _molecules():
-    yield syn.config0_water10(0)
+    yield syn.water10_cluster(0)
     for n, seed in [(3, 1), (12, 2), (40, 3)]:
         yield syn.attach_synthetic_basis(syn.organic_molecule(n, seed), aux_l_max=2, seed=seed)
 

@@ -51,7 +51,7 @@ def test_golden_case(name):
 
 @pytest.fixture(scope="module")
 def water10():
-    mol = syn.config0_water10(0)
+    mol = syn.water10_cluster(0)
     return mol, pu.form_pair_data(mol, 1e-14), pu.form_auxiliary_pair_data(mol)
 
 

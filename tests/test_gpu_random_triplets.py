@@ -21,7 +21,7 @@ lib = importlib.import_module("electron-integral-playground_b200._lib")
 
 @pytest.fixture(scope="module")
 def triplets():
-    return syn.config3_triplets(0, 2000)
+    return syn.random_shell_triplets(0, 2000)
 
 
 def test_boys_1e6_samples_against_series():
