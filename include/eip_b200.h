@@ -175,7 +175,7 @@ int eip_batch_add_charges(eip_batch* batch, int molecule, const double* position
  * where Q are Schwarz-type upper bounds built like the reference front end's
  * pair bound; every other shell pair stays FP64. */
 int eip_batch_set_precision(eip_batch* batch, int mode, double fp32_threshold);
-/* Number of streams (1..8, default 4) the class kernels of a run are forked
+/* Number of streams (1..8, default 1) the class kernels of a run are forked
  * over; set before the first run. */
 int eip_batch_set_streams(eip_batch* batch, int n_streams);
 int eip_batch_build(eip_batch* batch);
