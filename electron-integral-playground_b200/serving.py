@@ -17,7 +17,9 @@ asking for S, V, (P|Q) and (mu nu|P).  The server
 * batches the whole pieces admitted at one moment into ONE batch (one
   CUDA-graph launch over all their classes) on its own stream, and launches a
   window alone on its request's resident batch; up to `max_inflight` launches
-  overlap on the device;
+  are queued on the device (with `serialize`, the default, each waits on the
+  device for the previous one, so the GPU runs one batch at a time while the
+  next ones are built and queued);
 * when a launch completes, hands each of its pieces' packed class blocks
   (device views into the arena) to `consumer(request, piece, blocks)` on a
   consumer stream (default: a per-request digest, sum of squares, on the
@@ -205,7 +207,8 @@ def default_consumer(request, piece, blocks):
 
 class IntegralServer:
     def __init__(self, budget_bytes=150e9, precision="mixed", max_inflight=3, slice_fraction=0.25,
-                 consumer=default_consumer, host_overlap=True, keep_blocks=False, fp32_threshold=None):
+                 consumer=default_consumer, host_overlap=True, keep_blocks=False, fp32_threshold=None,
+                 serialize=True):
         import torch
 
         self.torch = torch
@@ -213,6 +216,12 @@ class IntegralServer:
         self.precision = precision
         self.fp32_threshold = fp32_threshold
         self.max_inflight = max_inflight
+        # serialize: each launch waits (on the device) for the previous one, so
+        # the GPU runs one batch at a time while later batches are built and
+        # queued; persistent kernels of different batches sharing the GPU slow
+        # each other down
+        self.serialize = serialize
+        self._last_ev = None
         self.slice_elems = int(self.arena.capacity * slice_fraction)
         self.consumer = consumer
         self.host_overlap = host_overlap
@@ -418,9 +427,11 @@ class IntegralServer:
             b.close()
             raise RuntimeError("packed output size differs from the planned size")
         b.bind_output(self.arena.buf.data_ptr() + 8 * off)
+        self._after_previous(b)
         b.run(sync=False)
         ev = torch.cuda.Event()
         ev.record(torch.cuda.ExternalStream(b.stream))
+        self._last_ev = ev
         self.launches += 1
         layout = [self._layout(p, lambda li, lj, lk, m=m: b.block(m, li, lj, lk)) for m, p in enumerate(group)]
         self.host_s["build"] += time.perf_counter() - tb
@@ -439,12 +450,19 @@ class IntegralServer:
         if n != piece.elems:
             raise RuntimeError("window output size differs from the planned size")
         layout = [self._layout(piece, lambda li, lj, lk: b.window_block(0, li, lj, lk))]
+        self._after_previous(b)
         b.run_window(self.arena.buf.data_ptr() + 8 * off)
         ev = torch.cuda.Event()
         ev.record(torch.cuda.ExternalStream(b.stream))
+        self._last_ev = ev
         self.launches += 1
         self.host_s["build"] += time.perf_counter() - tb
         return (b, ev, [piece], off, alloc, layout)
+
+    def _after_previous(self, b):
+        """With serialize, order b's next launch after the previous launch."""
+        if self.serialize and self._last_ev is not None:
+            self.torch.cuda.ExternalStream(b.stream).wait_event(self._last_ev)
 
     @staticmethod
     def _layout(piece, block_of):
