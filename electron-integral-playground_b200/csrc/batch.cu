@@ -20,6 +20,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <parallel/algorithm>
 #include <map>
 #include <numeric>
 #include <vector>
@@ -154,10 +155,13 @@ void group_indices(const int* ia, const int* ja, int n, std::vector<int>& order,
                    std::vector<int>& gi, std::vector<int>& gj) {
     order.resize(n);
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    auto less = [&](int x, int y) {
         const int jx = ja ? ja[x] : 0, jy = ja ? ja[y] : 0;
         return ia[x] != ia[y] ? ia[x] < ia[y] : jx < jy;
-    });
+    };
+    // large tables (a big molecule's pairs): the multi-threaded stable sort
+    if (n > (1 << 16)) __gnu_parallel::stable_sort(order.begin(), order.end(), less);
+    else std::stable_sort(order.begin(), order.end(), less);
     begin.clear();
     gi.clear();
     gj.clear();
