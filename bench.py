@@ -235,10 +235,22 @@ def run_serving(args, torch, seed):
     server.launches = 0
     st = server.serve(reqs, realtime=True)
     pieces = sum(len(server.pieces_of(r)) for r in reqs)
+    low = None
+    if args.serve_rate_low > 0:
+        # the same molecules arriving below the server's capacity: latency is
+        # then service time rather than queueing
+        t_low = np.cumsum(np.random.default_rng(seed + 13).exponential(1.0 / args.serve_rate_low, n))
+        server.launches = 0
+        sl = server.serve([sv.Request(i, m, arrival=float(t)) for i, (m, t) in enumerate(zip(mols, t_low))],
+                          realtime=True)
+        low = {"rate_rps": args.serve_rate_low, "throughput_rps": sl["throughput_rps"], "wall_s": sl["wall_s"],
+               "latency_p50_ms": sl["latency_p50_s"] * 1e3, "latency_p99_ms": sl["latency_p99_s"] * 1e3,
+               "launches": sl["launches"]}
     del server
     torch.cuda.empty_cache()
     alone = []
-    solo = sv.IntegralServer(budget_bytes=budget, precision="fp64", max_inflight=1, host_overlap=False)
+    # the same work per request as served (S included), nothing else in flight
+    solo = sv.IntegralServer(budget_bytes=budget, precision="fp64", max_inflight=1)
     for r in reqs[:args.serve_alone]:
         one = sv.Request(r.rid, r.molecule, arrival=0.0)
         alone.append(solo.serve([one], realtime=False)["latency_p50_s"])
@@ -251,11 +263,12 @@ def run_serving(args, torch, seed):
         "budget_gb": budget / 1e9, "precision": "mixed", "launches": st["launches"], "pieces": pieces,
         "throughput_rps": st["throughput_rps"], "wall_s": st["wall_s"], "host_s": st["host_s"],
         "latency_p50_ms": st["latency_p50_s"] * 1e3, "latency_p99_ms": st["latency_p99_s"] * 1e3,
+        "same_requests_below_capacity": low,
         "alone_fp64": {"requests": len(alone), "sum_s": float(lat_alone.sum()),
                        "throughput_rps": len(alone) / float(lat_alone.sum()),
                        "latency_p50_ms": float(np.percentile(lat_alone, 50)) * 1e3,
                        "latency_p99_ms": float(np.percentile(lat_alone, 99)) * 1e3,
-                       "note": "each request served alone (nothing else in flight), FP64"
+                       "note": "each request served alone (nothing else in flight), FP64, same work (S, V, (P|Q), (mu nu|P))"
                                + ("" if frac == 1 else f", first {len(alone)} requests")},
         "sample": f"{n} of the 10k-request stream (Poisson {args.serve_rate} req/s, 5-200 atoms log-uniform); "
                   "requests carry molecules, pair tables are built on the device after arrival",
@@ -391,6 +404,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=24, help="serving sample: requests (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="serving sample: Poisson arrival rate, req/s")
     ap.add_argument("--serve-alone", type=int, default=24, help="requests also timed alone in FP64")
+    ap.add_argument("--serve-rate-low", type=float, default=2.0,
+                    help="the same requests again at this Poisson rate (below capacity); 0 = skip")
     ap.add_argument("--no-config2", action="store_true",
                     help="skip the 100-water mixed-vs-FP64 per-class measurement")
     ap.add_argument("--tune", action="store_true",

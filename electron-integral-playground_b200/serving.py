@@ -233,6 +233,8 @@ class IntegralServer:
         self._dead = []
         # launches whose consumer work is queued: (event, off, alloc, pieces)
         self._consuming = []
+        # requests whose device pieces are done, waiting for S
+        self._awaiting_s = []
         self.cstream = torch.cuda.Stream()
         # host seconds spent planning pieces, building batches, retiring launches
         self.host_s = {"plan": 0.0, "build": 0.0, "retire": 0.0}
@@ -296,7 +298,10 @@ class IntegralServer:
             req = q.get()
             if req is None:
                 return
-            req.S = overlap(req.pair_data, req.molecule)
+            try:
+                req.S = overlap(req.pair_data, req.molecule)
+            except Exception as exc:  # reported by the loop, which must not wait forever
+                req.S = exc
 
     # -- the loop ------------------------------------------------------------------
     def serve(self, requests, realtime=True):
@@ -359,6 +364,8 @@ class IntegralServer:
                     if entry[0].query():
                         self._consumed(entry, finished, t0)
                         self._consuming.remove(entry)
+                if self._awaiting_s:
+                    self._finish_ready(finished, t0)
                 if self._dead and ((not inflight and not self._consuming) or len(self._dead) > 64):
                     self._close_dead()
                 if waiting and len(inflight) < self.max_inflight:
@@ -505,16 +512,25 @@ class IntegralServer:
 
     def _consumed(self, entry, finished, t0):
         """The consumer's work on a launch's output has finished: free the arena
-        range; a request is done when its last piece is."""
+        range; a request is done when its last piece is and its S (worker
+        thread) is ready."""
         _, off, alloc, pieces = entry
         self.arena.release(off, alloc)
         for p in pieces:
             p.request.pieces_left -= 1
             if p.request.pieces_left == 0:
-                p.request.done = time.perf_counter() - t0
                 if p.request.digest_dev is not None:
                     p.request.digest = float(p.request.digest_dev)
-                finished.append(p.request)
+                self._awaiting_s.append(p.request)
+        self._finish_ready(finished, t0)
+
+    def _finish_ready(self, finished, t0):
+        for req in [r for r in self._awaiting_s if r.S is not None or not self.host_overlap]:
+            if isinstance(req.S, Exception):
+                raise RuntimeError(f"request {req.rid}: overlap failed") from req.S
+            self._awaiting_s.remove(req)
+            req.done = time.perf_counter() - t0
+            finished.append(req)
 
     def _close_dead(self):
         """Check the self-check words of finished batches and destroy them."""
