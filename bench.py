@@ -232,9 +232,16 @@ def run_serving(args, torch, seed):
     server = sv.IntegralServer(budget_bytes=budget, precision="mixed", fp32_threshold=args.fp32_threshold)
     warm = sv.Request(-1, mols[0], arrival=0.0)
     server.serve([warm], realtime=False)
-    server.launches = 0
-    st = server.serve(reqs, realtime=True)
-    pieces = sum(len(server.pieces_of(r)) for r in reqs)
+    # the host side (threads, builds) makes single runs vary: serve the same
+    # stream several times (fresh requests) and report the median run
+    runs = []
+    for _ in range(max(1, args.serve_repeats)):
+        server.launches = 0
+        server.host_s = {k: 0.0 for k in server.host_s}
+        fresh = [sv.Request(r.rid, r.molecule, arrival=r.arrival) for r in reqs]
+        runs.append(server.serve(fresh, realtime=True))
+    st = sorted(runs, key=lambda x: x["throughput_rps"])[len(runs) // 2]
+    pieces = sum(len(server.pieces_of(r)) for r in fresh)  # fresh: the last run's requests, tables built
     low = None
     if args.serve_rate_low > 0:
         # the same molecules arriving below the server's capacity: latency is
@@ -262,6 +269,7 @@ def run_serving(args, torch, seed):
         "requests": n, "rate_rps": args.serve_rate, "atoms": [int(x) for x in sizes],
         "budget_gb": budget / 1e9, "precision": "mixed", "launches": st["launches"], "pieces": pieces,
         "throughput_rps": st["throughput_rps"], "wall_s": st["wall_s"], "host_s": st["host_s"],
+        "runs_throughput_rps": [r["throughput_rps"] for r in runs], "runs_note": "median run reported",
         "latency_p50_ms": st["latency_p50_s"] * 1e3, "latency_p99_ms": st["latency_p99_s"] * 1e3,
         "same_requests_below_capacity": low,
         "alone_fp64": {"requests": len(alone), "sum_s": float(lat_alone.sum()),
@@ -404,6 +412,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=24, help="serving sample: requests (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="serving sample: Poisson arrival rate, req/s")
     ap.add_argument("--serve-alone", type=int, default=24, help="requests also timed alone in FP64")
+    ap.add_argument("--serve-repeats", type=int, default=3, help="serving runs of the stream (median reported)")
     ap.add_argument("--serve-rate-low", type=float, default=2.0,
                     help="the same requests again at this Poisson rate (below capacity); 0 = skip")
     ap.add_argument("--no-config2", action="store_true",
