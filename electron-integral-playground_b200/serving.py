@@ -1,7 +1,9 @@
 """Continuous-batching integral server (device-resident request loop).
 
-A request is one molecule (its pair and auxiliary tables, the C-ABI formats)
-asking for S, V, (P|Q) and (mu nu|P).  The server
+A request is one molecule asking for S, V, (P|Q) and (mu nu|P); it may carry
+its pair and auxiliary tables (the C-ABI formats) or leave them to the server,
+which builds them after arrival (pair tables on the device, on builder
+threads).  The server
 
 * splits each request into device pieces: (mu nu|P) with V (one slot: the
   pair tables against the auxiliary basis and against the nuclei as
@@ -27,7 +29,8 @@ asking for S, V, (P|Q) and (mu nu|P).  The server
   finished — the loop never waits for it; S comes from the drop-in overlap
   entry point on a worker thread while the GPU works.
 
-Latency of a request = completion of its last piece minus its arrival.
+Latency of a request = the later of its last piece's consumption and its S,
+minus its arrival.
 Precision "mixed" uses the batch's FP32 gate for (mu nu|P) (<= 1e-10 of FP64,
 tested); V and (P|Q) are always FP64.
 """
@@ -41,6 +44,7 @@ import time
 import numpy as np
 
 from .batch import POINT_CHARGES, ThreeCenterBatch, metric_pair_tables
+
 
 def aux_slices(aux_data, n_aux, max_functions):
     """Split the auxiliary tables into slices of whole shells, at most
