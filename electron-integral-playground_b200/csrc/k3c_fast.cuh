@@ -21,6 +21,8 @@
 //   * E^{ij}_t tables of each primitive pair are precomputed once into the
 //     device-resident pair table (e_table_kernel) and staged per pair into
 //     shared memory;
+//   * one-warp CTAs (most low-l classes) keep the unit's Boys values in
+//     registers and load the next unit's data while evaluating the current one;
 //   * primitive pairs are reduced in registers: each contracted block is
 //     written once, with no atomics.
 // Packed output of molecule m (element offset out_begin[m]):
@@ -63,7 +65,7 @@ struct Fast3c {
     static constexpr int NU = L + 6;
     template <typename T>
     static constexpr size_t smem_bytes() {
-        return sizeof(double) * UB * NU * 32 + sizeof(T) * (NR * 32 + UB * 3 * NE);
+        return (KS == 1 ? 0 : sizeof(double) * UB * NU * 32) + sizeof(T) * (NR * 32 + UB * 3 * NE);
     }
 };
 
@@ -153,6 +155,35 @@ __global__ void e_table_kernel(BraTable bra, double* __restrict__ prim_E) {
     }
 }
 
+// Exponent zeta of the Boys argument and the prefactor of one unit: a primitive
+// pair of exponent p and an auxiliary primitive of exponent q, c the product
+// of their coefficients (MI/three_center.cpp:46-49 and, for POINT,
+// MI/nuclear_attraction.cpp:44-45, 69).  omega == 0 uses one division:
+// t = 1/(pq(p+q)), zeta = (pq)^2 t, prefactor = c 2 pi^{5/2} sqrt(p+q) t.
+template <int LK, bool POINT>
+__device__ __forceinline__ void unit_prefactor(double p, double q, double c, double omega, double& zeta,
+                                               double& pref) {
+    if constexpr (POINT) {
+        static_assert(LK == 0, "point charges have no angular momentum");
+        if (omega == 0.0) {
+            zeta = p;
+            pref = c * 2.0 * kPi / p;
+        } else {
+            zeta = p * omega * omega / (p + omega * omega);
+            pref = c * 2.0 * kPi * omega / (p * sqrt(p + omega * omega));
+        }
+    } else if (omega == 0.0) {
+        const double pq = p * q, s = p + q;
+        const double t = 1.0 / (pq * s);
+        zeta = pq * pq * t;
+        pref = c * kTwoPi52 * sqrt(s) * t;
+    } else {
+        zeta = 1.0 / (1.0 / p + 1.0 / q + 1.0 / (omega * omega));
+        pref = c * kTwoPi52 * omega / (p * q * sqrt(p * q + (p + q) * omega * omega));
+    }
+    if (LK & 1) pref = -pref;  // (-1)^{|s|} with |s| = LK mod 2
+}
+
 // T: arithmetic type of the R tetrahedron, ket, bra and accumulation (double,
 // or float for the mixed-precision path).  Boys, R^{(m)}_000, the E^{ij}_t
 // recurrences (precomputed in FP64) and the prefactors are FP64 in both.
@@ -170,10 +201,11 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
     constexpr int NU = C::NU;
     // dynamic shared memory (fast3c_smem_bytes): per block of UB units
     // (primitive pair x auxiliary primitive) the lanes' R^(m)_000 and unit
-    // data, then the R tetrahedron of the current unit, then the units' E tables
+    // data (CTAs of several warps only), then the R tetrahedron of the current
+    // unit, then the units' E tables
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* sU = reinterpret_cast<double*>(smem_raw);  // [UB][NU][32]
-    T* sR = reinterpret_cast<T*>(sU + UB * NU * 32);    // [NR][32]
+    double* sU = reinterpret_cast<double*>(smem_raw);                   // [UB][NU][32], KS > 1
+    T* sR = reinterpret_cast<T*>(sU + (C::KS == 1 ? 0 : UB * NU * 32));  // [NR][32]
     T* sE = sR + C::NR * 32;                            // [UB][3 NE]
     __shared__ int s_item;
 
@@ -246,72 +278,114 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
         // units one by one, splitting each unit's R tetrahedron and ket
         // components between them.
         const int n_units = (pe - pb) * nk_max;
+        // One-warp CTAs (KS == 1) keep a unit's values in registers and load
+        // the next unit's primitive data and E table while the current unit is
+        // evaluated, so a unit's global loads are off its dependency chain;
+        // warp barriers replace block barriers.
+        constexpr int NE3 = 3 * C::NE;
+        constexpr bool ONE = C::KS == 1;
+        constexpr int EPL = ONE ? (NE3 + 31) / 32 : 1;  // E values per lane
+        double4 nP, nPA, nC;
+        double ncc, nE[EPL];
+        bool nlive = false;
+        auto fetch = [&](int u) {
+            const int pp = pb + u / nk_max, kk = u - (u / nk_max) * nk_max;
+            nP = bra.prim_P[pp];
+            nPA = bra.prim_PA[pp];
+            nlive = kk < nk;
+            nC = nlive ? ket.prim_C[kb + kk] : make_double4(0.0, 0.0, 0.0, 1.0);
+            ncc = nlive ? ket.prim_coef[kb + kk] : 0.0;
+#pragma unroll
+            for (int r = 0; r < EPL; r++) {
+                const int e = lane + 32 * r;
+                nE[r] = e < NE3 ? __ldg(bra.prim_E + (size_t)pp * NE3 + e) : 0.0;
+            }
+        };
+        if constexpr (ONE) {
+            if (n_units > 0) fetch(0);
+        }
+        double uRm[ONE ? L + 1 : 1], uX = 0.0, uY = 0.0, uZ = 0.0, upref = 0.0, uq = 1.0, uinv2q = 0.5;
         for (int u0 = 0; u0 < n_units; u0 += UB) {
             const int nb = n_units - u0 < UB ? n_units - u0 : UB;
-            for (int e = threadIdx.x; e < nb * 3 * C::NE; e += C::THREADS) {
-                const int ub = e / (3 * C::NE), r = e - ub * (3 * C::NE);
-                const int pp = pb + (u0 + ub) / nk_max;
-                sE[e] = (T)__ldg(bra.prim_E + (size_t)pp * 3 * C::NE + r);
-            }
-            for (int ub = warp; ub < nb; ub += C::KS) {
-                const int u = u0 + ub;
-                const int pp = pb + u / nk_max, kk = u - (u / nk_max) * nk_max;
-                const double4 P = bra.prim_P[pp];
-                const double4 PA = bra.prim_PA[pp];
-                const double p = P.w;
-                const bool live = kk < nk;
-                const double4 Cq = live ? ket.prim_C[kb + kk] : make_double4(P.x, P.y, P.z, 1.0);
-                const double cc = live ? ket.prim_coef[kb + kk] : 0.0;
-                const double q = Cq.w;
-                const double X = P.x - Cq.x, Y = P.y - Cq.y, Z = P.z - Cq.z;
-                double zeta, pref64;
-                if constexpr (POINT) {
-                    static_assert(LK == 0, "point charges have no angular momentum");
-                    if (omega == 0.0) {
-                        zeta = p;
-                        pref64 = PA.w * cc * 2.0 * kPi / p;
-                    } else {
-                        zeta = p * omega * omega / (p + omega * omega);
-                        pref64 = PA.w * cc * 2.0 * kPi * omega / (p * sqrt(p + omega * omega));
-                    }
-                } else if (omega == 0.0) {
-                    zeta = p * q / (p + q);
-                    pref64 = PA.w * cc * kTwoPi52 / (p * q * sqrt(p + q));
-                } else {
-                    zeta = 1.0 / (1.0 / p + 1.0 / q + 1.0 / (omega * omega));
-                    pref64 = PA.w * cc * kTwoPi52 * omega / (p * q * sqrt(p * q + (p + q) * omega * omega));
-                }
-                if (LK & 1) pref64 = -pref64;  // (-1)^{|s|} with |s| = LK mod 2
-                // R^{(m)}_000 = (-2 zeta)^m F_m(zeta |PQ|^2)
-                double Rm[L + 1];
-                boys<L>(boys_table, zeta * (X * X + Y * Y + Z * Z), Rm);
-                double* unit = sU + ub * NU * 32 + lane;
-                const double f = -2.0 * zeta;
-                double g = 1.0;
+            if constexpr (ONE) {
+                const double4 P = nP, PA = nPA;
+                const double4 Cq = nlive ? nC : make_double4(P.x, P.y, P.z, 1.0);
+                const double cc = ncc;
 #pragma unroll
-                for (int mm = 0; mm <= L; mm++) {
-                    unit[mm * 32] = Rm[mm] * g;
+                for (int r = 0; r < EPL; r++)
+                    if (lane + 32 * r < NE3) sE[lane + 32 * r] = (T)nE[r];
+                if (u0 + 1 < n_units) fetch(u0 + 1);
+                uX = P.x - Cq.x;
+                uY = P.y - Cq.y;
+                uZ = P.z - Cq.z;
+                // with uncontracted auxiliary shells (nk_max == 1) every unit of
+                // the item has the lane's same q
+                if (u0 == 0 || nk_max > 1) {
+                    uq = Cq.w;
+                    uinv2q = 0.5 / uq;
+                }
+                double zeta;
+                unit_prefactor<LK, POINT>(P.w, uq, PA.w * cc, omega, zeta, upref);
+                // R^{(m)}_000 = (-2 zeta)^m F_m(zeta |PQ|^2)
+                boys<L>(boys_table, zeta * (uX * uX + uY * uY + uZ * uZ), uRm);
+                const double f = -2.0 * zeta;
+                double g = f;
+#pragma unroll
+                for (int mm = 1; mm <= L; mm++) {
+                    uRm[mm] *= g;
                     g *= f;
                 }
-                unit[(L + 1) * 32] = X;
-                unit[(L + 2) * 32] = Y;
-                unit[(L + 3) * 32] = Z;
-                unit[(L + 4) * 32] = pref64;
-                unit[(L + 5) * 32] = q;
+            } else {
+                for (int e = threadIdx.x; e < nb * NE3; e += C::THREADS) {
+                    const int ub = e / NE3, r = e - ub * NE3;
+                    const int pp = pb + (u0 + ub) / nk_max;
+                    sE[e] = (T)__ldg(bra.prim_E + (size_t)pp * NE3 + r);
+                }
+                for (int ub = warp; ub < nb; ub += C::KS) {
+                    const int u = u0 + ub;
+                    const int pp = pb + u / nk_max, kk = u - (u / nk_max) * nk_max;
+                    const double4 P = bra.prim_P[pp];
+                    const double4 PA = bra.prim_PA[pp];
+                    const bool live = kk < nk;
+                    const double4 Cq = live ? ket.prim_C[kb + kk] : make_double4(P.x, P.y, P.z, 1.0);
+                    const double cc = live ? ket.prim_coef[kb + kk] : 0.0;
+                    const double q = Cq.w;
+                    const double X = P.x - Cq.x, Y = P.y - Cq.y, Z = P.z - Cq.z;
+                    double zeta, pref64;
+                    unit_prefactor<LK, POINT>(P.w, q, PA.w * cc, omega, zeta, pref64);
+                    // R^{(m)}_000 = (-2 zeta)^m F_m(zeta |PQ|^2)
+                    double Rm[L + 1];
+                    boys<L>(boys_table, zeta * (X * X + Y * Y + Z * Z), Rm);
+                    double* unit = sU + ub * NU * 32 + lane;
+                    const double f = -2.0 * zeta;
+                    double g = 1.0;
+#pragma unroll
+                    for (int mm = 0; mm <= L; mm++) {
+                        unit[mm * 32] = Rm[mm] * g;
+                        g *= f;
+                    }
+                    unit[(L + 1) * 32] = X;
+                    unit[(L + 2) * 32] = Y;
+                    unit[(L + 3) * 32] = Z;
+                    unit[(L + 4) * 32] = pref64;
+                    unit[(L + 5) * 32] = q;
+                }
+                __syncthreads();
             }
-            __syncthreads();
             for (int ub = 0; ub < nb; ub++) {
                 const double* unit = sU + ub * NU * 32 + lane;
-                const T* sEu = sE + ub * (3 * C::NE);
-                const double X = unit[(L + 1) * 32], Y = unit[(L + 2) * 32], Z = unit[(L + 3) * 32];
-                const T pref = (T)unit[(L + 4) * 32];
-                const double q = unit[(L + 5) * 32];
+                const T* sEu = sE + ub * NE3;
+                const double X = ONE ? uX : unit[(L + 1) * 32];
+                const double Y = ONE ? uY : unit[(L + 2) * 32];
+                const double Z = ONE ? uZ : unit[(L + 3) * 32];
+                const T pref = (T)(ONE ? upref : unit[(L + 4) * 32]);
+                const double q = ONE ? uq : unit[(L + 5) * 32];
                 // this warp's share of the tetrahedron by the closed form
                 // (entries are independent)
                 T Rt[L + 1], px[L + 1], py[L + 1], pz[L + 1];
                 px[0] = py[0] = pz[0] = T(1);
 #pragma unroll
-                for (int mm = 0; mm <= L; mm++) Rt[mm] = (T)unit[mm * 32];
+                for (int mm = 0; mm <= L; mm++) Rt[mm] = (T)(ONE ? uRm[ONE ? mm : 0] : unit[mm * 32]);
 #pragma unroll
                 for (int mm = 1; mm <= L; mm++) {
                     px[mm] = px[mm - 1] * (T)X;
@@ -351,7 +425,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 // (1/2q)^{LK - j}: weight of the ket terms with |s| = LK - 2j
                 T w[LK / 2 + 1];
                 {
-                    const double inv2q = 0.5 / q;
+                    const double inv2q = ONE ? uinv2q : 0.5 / q;
                     double base = 1.0;
 #pragma unroll
                     for (int j = 0; j < LK - LK / 2; j++) base *= inv2q;
@@ -361,7 +435,8 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                         base *= inv2q;
                     }
                 }
-                __syncthreads();
+                if constexpr (ONE) __syncwarp();
+                else __syncthreads();
 
                 // ket + bra.  Warp w owns ket components ko = w * KPW + c, c < KPW.
                 // One warp per CTA: ket coefficients are compile-time constants
@@ -474,7 +549,8 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                             acc[ci * C::NJ + cj][c] = fma(pref, sxv[c], acc[ci * C::NJ + cj][c]);
                     });
                 });
-                __syncthreads();
+                if constexpr (ONE) __syncwarp();
+                else __syncthreads();
             }
         }
 
