@@ -285,36 +285,41 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
         constexpr int NE3 = 3 * C::NE;
         constexpr bool ONE = C::KS == 1;
         constexpr int EPL = ONE ? (NE3 + 31) / 32 : 1;  // E values per lane
-        double4 nP, nPA, nC;
-        double ncc, nE[EPL];
+        double4 nP, nC;
+        double nca = 0.0, ncc = 0.0, nE[EPL];
         bool nlive = false;
-        auto fetch = [&](int u) {
-            const int pp = pb + u / nk_max, kk = u - (u / nk_max) * nk_max;
-            nP = bra.prim_P[pp];
-            nPA = bra.prim_PA[pp];
-            nlive = kk < nk;
-            nC = nlive ? ket.prim_C[kb + kk] : make_double4(0.0, 0.0, 0.0, 1.0);
-            ncc = nlive ? ket.prim_coef[kb + kk] : 0.0;
+        // units are fetched in order: primitive pair fpp, auxiliary primitive fkk
+        int fpp = pb, fkk = 0;
+        auto fetch = [&]() {
+            nP = bra.prim_P[fpp];
+            nca = bra.prim_PA[fpp].w;
+            nlive = fkk < nk;
+            nC = nlive ? ket.prim_C[kb + fkk] : make_double4(0.0, 0.0, 0.0, 1.0);
+            ncc = nlive ? ket.prim_coef[kb + fkk] : 0.0;
 #pragma unroll
             for (int r = 0; r < EPL; r++) {
                 const int e = lane + 32 * r;
-                nE[r] = e < NE3 ? __ldg(bra.prim_E + (size_t)pp * NE3 + e) : 0.0;
+                nE[r] = e < NE3 ? __ldg(bra.prim_E + (size_t)fpp * NE3 + e) : 0.0;
+            }
+            if (++fkk == nk_max) {
+                fkk = 0;
+                fpp++;
             }
         };
         if constexpr (ONE) {
-            if (n_units > 0) fetch(0);
+            if (n_units > 0) fetch();
         }
         double uRm[ONE ? L + 1 : 1], uX = 0.0, uY = 0.0, uZ = 0.0, upref = 0.0, uq = 1.0, uinv2q = 0.5;
         for (int u0 = 0; u0 < n_units; u0 += UB) {
             const int nb = n_units - u0 < UB ? n_units - u0 : UB;
             if constexpr (ONE) {
-                const double4 P = nP, PA = nPA;
+                const double4 P = nP;
                 const double4 Cq = nlive ? nC : make_double4(P.x, P.y, P.z, 1.0);
-                const double cc = ncc;
+                const double c = nca * ncc;
 #pragma unroll
                 for (int r = 0; r < EPL; r++)
                     if (lane + 32 * r < NE3) sE[lane + 32 * r] = (T)nE[r];
-                if (u0 + 1 < n_units) fetch(u0 + 1);
+                if (u0 + 1 < n_units) fetch();
                 uX = P.x - Cq.x;
                 uY = P.y - Cq.y;
                 uZ = P.z - Cq.z;
@@ -325,7 +330,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                     uinv2q = 0.5 / uq;
                 }
                 double zeta;
-                unit_prefactor<LK, POINT>(P.w, uq, PA.w * cc, omega, zeta, upref);
+                unit_prefactor<LK, POINT>(P.w, uq, c, omega, zeta, upref);
                 // R^{(m)}_000 = (-2 zeta)^m F_m(zeta |PQ|^2)
                 boys<L>(boys_table, zeta * (uX * uX + uY * uY + uZ * uZ), uRm);
                 const double f = -2.0 * zeta;
