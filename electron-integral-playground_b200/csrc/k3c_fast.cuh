@@ -343,12 +343,13 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
             } else {
                 for (int e = threadIdx.x; e < nb * NE3; e += C::THREADS) {
                     const int ub = e / NE3, r = e - ub * NE3;
-                    const int pp = pb + (u0 + ub) / nk_max;
+                    const int pp = pb + (nk_max == 1 ? u0 + ub : (u0 + ub) / nk_max);
                     sE[e] = (T)__ldg(bra.prim_E + (size_t)pp * NE3 + r);
                 }
                 for (int ub = warp; ub < nb; ub += C::KS) {
                     const int u = u0 + ub;
-                    const int pp = pb + u / nk_max, kk = u - (u / nk_max) * nk_max;
+                    const int up = nk_max == 1 ? u : u / nk_max;  // uncontracted auxiliary shells: no division
+                    const int pp = pb + up, kk = u - up * nk_max;
                     const double4 P = bra.prim_P[pp];
                     const double4 PA = bra.prim_PA[pp];
                     const bool live = kk < nk;
