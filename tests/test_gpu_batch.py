@@ -96,6 +96,69 @@ def test_every_tuning_variant_matches_reference(small_batch):
                 L.eip_tune_set(*k, v)
 
 
+def _contracted_auxiliary_molecule():
+    """A 5-atom molecule whose auxiliary shells (s-g, 3 per l and element) are
+    contractions of 1-4 primitives, so the 32 shells of a warp have ragged
+    primitive counts (units past a shell's own count contribute nothing)."""
+    basis_utility = importlib.import_module("electron-integral-playground_b200.basis_utility")
+    readers = importlib.import_module("electron-integral-playground_b200.readers")
+    rng = np.random.default_rng(31)
+    ladder = [0.1 * 2.5 ** i for i in range(9)]
+    lines = []
+    for el in ("C", "H", "N", "O"):
+        lines.append(f"{el}     0")
+        for l in range(5):
+            for _ in range(3):
+                k = int(rng.integers(1, 5))
+                exps = sorted(rng.choice(ladder, size=k, replace=False), reverse=True)
+                lines.append(f"{basis_utility.ANGULAR_LETTERS[l]}    {k}   1.00")
+                for e in exps:
+                    lines.append(f"    {float(e)!r}    {float(rng.uniform(0.2, 1.0))!r}")
+        lines.append("****")
+    m = syn.organic_molecule(5, seed=40)
+    m.spherical_basis = True
+    basis_utility.attach_basis_to_molecule(m, readers.read_basis_content(syn.orbital_basis_text(["H", "C", "N", "O"], 3)))
+    basis_utility.attach_auxiliary_basis_to_molecule(m, readers.read_basis_content("\n".join(lines) + "\n"))
+    return m
+
+
+def test_contracted_auxiliary_every_variant_and_mixed():
+    """Contracted, ragged auxiliary shells through every launch variant of the
+    fast kernels (one-warp and multi-warp CTAs) and through a mixed batch,
+    against the reference library."""
+    ref = oracle.reference()
+    if ref is None:
+        pytest.skip("reference library not built")
+    m = _contracted_auxiliary_molecule()
+    pd, ad = pu.form_pair_data(m, 1e-14), pu.form_auxiliary_pair_data(m)
+    counts = np.concatenate([np.unique(a.i_ao_start, return_counts=True)[1] for a in ad.values()])
+    assert counts.max() > 1 and counts.min() == 1  # ragged contractions
+    want = oracle.drive_three_center(ref, pd, ad, m)
+    lm = importlib.import_module("electron-integral-playground_b200._lib")
+    L = lm.lib()
+    saved = {(li, lj, lk): L.eip_tune_get(li, lj, lk) for (li, lj) in pd for lk in ad}
+    try:
+        for v in range(6):
+            for (li, lj, lk) in saved:
+                if saved[(li, lj, lk)] >= 0:
+                    L.eip_tune_set(li, lj, lk, v)
+            got = mi.three_center(pd, ad, m)
+            np.testing.assert_allclose(got, want, rtol=0, atol=1e-12, err_msg=f"variant {v}")
+    finally:
+        for k, v in saved.items():
+            if v >= 0:
+                L.eip_tune_set(*k, v)
+    mix = bt.ThreeCenterBatch([m], [pd], [ad], precision="mixed", fp32_threshold=float("inf"))
+    mix.alloc_output()
+    mix.run()
+    mix.status()
+    err = np.max(np.abs(mix.dense(0) - want))
+    mix.close()
+    # every shell pair in FP32 (R, ket, bra): a loose bound that still catches
+    # any misplaced component or unit
+    assert 0.0 < err <= 1e-4 * max(1.0, float(np.max(np.abs(want)))), err
+
+
 def _two_fragments():
     ds = importlib.import_module("electron-integral-playground_b200.data_structure")
     a = syn.organic_molecule(6, seed=21)
