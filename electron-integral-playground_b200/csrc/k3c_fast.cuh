@@ -445,48 +445,109 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 else __syncthreads();
 
                 // ket + bra.  Warp w owns ket components ko = w * KPW + c, c < KPW.
-                // One warp per CTA: ket coefficients are compile-time constants
-                // (zero terms vanish).  Several warps: the same code in every
-                // warp, coefficients from constant memory, so the instruction
-                // cache holds one copy.  Either way X[c][h] is formed for all
-                // c first, so each E^{ij}_t shared-memory load feeds KPW FMAs.
-                T Xh[C::KPW][C::NHB];
+                // X[c][h] is formed for a set of components first, so that each
+                // E^{ij}_t shared-memory load of the bra feeds one FMA per component.
+                // bra: acc[ij][c0 + c] += pref * sum_t Ex sum_u Ey sum_v Ez X[c][tuv], c < NC
+                auto bra_acc = [&](const auto& X, auto c0_, auto nc_) {
+                    constexpr int c0 = decltype(c0_)::value, NC = decltype(nc_)::value;
+                    static_for<0, C::NI>([&](auto ci_) {
+                        constexpr int ci = decltype(ci_)::value;
+                        constexpr int ix = cart_x(LI, ci), iy = cart_y(LI, ci), iz = cart_z(LI, ci);
+                        static_for<0, C::NJ>([&](auto cj_) {
+                            constexpr int cj = decltype(cj_)::value;
+                            constexpr int jx = cart_x(LJ, cj), jy = cart_y(LJ, cj), jz = cart_z(LJ, cj);
+                            T sxv[NC];
 #pragma unroll
-                for (int c = 0; c < C::KPW; c++)
+                            for (int c = 0; c < NC; c++) sxv[c] = T(0);
+                            static_for<0, ix + jx + 1>([&](auto t_) {
+                                constexpr int t = decltype(t_)::value;
+                                T su[NC];
 #pragma unroll
-                    for (int h = 0; h < C::NHB; h++) Xh[c][h] = T(0);
-                if constexpr (C::KS == 1) {
-                    static_for<0, C::NHB>([&](auto h_) {
-                        constexpr int h = decltype(h_)::value;
-                        constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
-                        static_for<0, LK / 2 + 1>([&](auto j_) {
-                            constexpr int j = decltype(j_)::value;
-                            constexpr int S = LK - 2 * j;
-                            T part[C::KPW];
+                                for (int c = 0; c < NC; c++) su[c] = T(0);
+                                static_for<0, iy + jy + 1>([&](auto u_) {
+                                    constexpr int u = decltype(u_)::value;
+                                    T sv[NC];
 #pragma unroll
-                            for (int c = 0; c < C::KPW; c++) part[c] = T(0);
-                            static_for<0, ncart(S)>([&](auto sc_) {
-                                constexpr int sc = decltype(sc_)::value;
-                                constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
-                                constexpr bool any = [] {
-                                    for (int c = 0; c < C::NKO; c++)
-                                        if (ket_sph_coef(LK, c, sx, sy, sz) != 0.0) return true;
-                                    return false;
-                                }();
-                                if constexpr (any) {
-                                    const T r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
-                                    static_for<0, C::NKO>([&](auto c_) {
-                                        constexpr int c = decltype(c_)::value;
-                                        constexpr double kc = ket_sph_coef(LK, c, sx, sy, sz);
-                                        if constexpr (kc != 0.0) part[c] = fma((T)kc, r, part[c]);
+                                    for (int c = 0; c < NC; c++) sv[c] = T(0);
+                                    static_for<0, iz + jz + 1>([&](auto v_) {
+                                        constexpr int v = decltype(v_)::value;
+                                        const T ez = sEu[2 * C::NE + e_offset<LJ>(iz, jz) + v];
+#pragma unroll
+                                        for (int c = 0; c < NC; c++) sv[c] = fma(ez, X[c][herm_index(t, u, v)], sv[c]);
                                     });
-                                }
+                                    const T ey = sEu[C::NE + e_offset<LJ>(iy, jy) + u];
+#pragma unroll
+                                    for (int c = 0; c < NC; c++) su[c] = fma(ey, sv[c], su[c]);
+                                });
+                                const T ex = sEu[e_offset<LJ>(ix, jx) + t];
+#pragma unroll
+                                for (int c = 0; c < NC; c++) sxv[c] = fma(ex, su[c], sxv[c]);
                             });
 #pragma unroll
-                            for (int c = 0; c < C::KPW; c++) Xh[c][h] = fma(w[j], part[c], Xh[c][h]);
+                            for (int c = 0; c < NC; c++)
+                                acc[ci * C::NJ + cj][c0 + c] = fma(pref, sxv[c], acc[ci * C::NJ + cj][c0 + c]);
                         });
                     });
+                };
+                if constexpr (C::KS == 1) {
+                    // One warp per CTA (KPW = NKO): ket coefficients are compile-time
+                    // constants (zero terms vanish).  When X[KPW][NHB] would hold
+                    // more than kXMax values, the components go in chunks (fewer
+                    // live registers; an R entry is loaded once per chunk).
+                    constexpr int kXMax = 48;
+                    constexpr int NCH = (C::KPW * C::NHB + kXMax - 1) / kXMax;
+                    constexpr int KCH = (C::KPW + NCH - 1) / NCH;
+                    static_for<0, (C::KPW + KCH - 1) / KCH>([&](auto q_) {
+                        constexpr int c0 = decltype(q_)::value * KCH;
+                        constexpr int NC = C::KPW - c0 < KCH ? C::KPW - c0 : KCH;
+                        // keep the compiler from holding the previous chunk's R
+                        // values in registers for this one
+                        if constexpr (c0 > 0) asm volatile("" ::: "memory");
+                        T Xh[NC][C::NHB];
+#pragma unroll
+                        for (int c = 0; c < NC; c++)
+#pragma unroll
+                            for (int h = 0; h < C::NHB; h++) Xh[c][h] = T(0);
+                        static_for<0, C::NHB>([&](auto h_) {
+                            constexpr int h = decltype(h_)::value;
+                            constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
+                            static_for<0, LK / 2 + 1>([&](auto j_) {
+                                constexpr int j = decltype(j_)::value;
+                                constexpr int S = LK - 2 * j;
+                                T part[NC];
+#pragma unroll
+                                for (int c = 0; c < NC; c++) part[c] = T(0);
+                                static_for<0, ncart(S)>([&](auto sc_) {
+                                    constexpr int sc = decltype(sc_)::value;
+                                    constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
+                                    constexpr bool any = [] {
+                                        for (int c = c0; c < c0 + NC; c++)
+                                            if (ket_sph_coef(LK, c, sx, sy, sz) != 0.0) return true;
+                                        return false;
+                                    }();
+                                    if constexpr (any) {
+                                        const T r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
+                                        static_for<0, NC>([&](auto c_) {
+                                            constexpr int c = decltype(c_)::value;
+                                            constexpr double kc = ket_sph_coef(LK, c0 + c, sx, sy, sz);
+                                            if constexpr (kc != 0.0) part[c] = fma((T)kc, r, part[c]);
+                                        });
+                                    }
+                                });
+#pragma unroll
+                                for (int c = 0; c < NC; c++) Xh[c][h] = fma(w[j], part[c], Xh[c][h]);
+                            });
+                        });
+                        bra_acc(Xh, ic<c0>{}, ic<NC>{});
+                    });
                 } else {
+                    // Several warps: the same code in every warp, coefficients
+                    // from constant memory, so the instruction cache holds one copy.
+                    T Xh[C::KPW][C::NHB];
+#pragma unroll
+                    for (int c = 0; c < C::KPW; c++)
+#pragma unroll
+                        for (int h = 0; h < C::NHB; h++) Xh[c][h] = T(0);
                     int sidx = 0;
                     static_for<0, LK / 2 + 1>([&](auto j_) {
                         constexpr int j = decltype(j_)::value;
@@ -515,46 +576,8 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                         });
                         sidx += ncart(S);
                     });
+                    bra_acc(Xh, ic<0>{}, ic<C::KPW>{});
                 }
-                // bra: acc[ij][c] += pref * sum_t Ex sum_u Ey sum_v Ez X[c][tuv]
-                static_for<0, C::NI>([&](auto ci_) {
-                    constexpr int ci = decltype(ci_)::value;
-                    constexpr int ix = cart_x(LI, ci), iy = cart_y(LI, ci), iz = cart_z(LI, ci);
-                    static_for<0, C::NJ>([&](auto cj_) {
-                        constexpr int cj = decltype(cj_)::value;
-                        constexpr int jx = cart_x(LJ, cj), jy = cart_y(LJ, cj), jz = cart_z(LJ, cj);
-                        T sxv[C::KPW];
-#pragma unroll
-                        for (int c = 0; c < C::KPW; c++) sxv[c] = T(0);
-                        static_for<0, ix + jx + 1>([&](auto t_) {
-                            constexpr int t = decltype(t_)::value;
-                            T su[C::KPW];
-#pragma unroll
-                            for (int c = 0; c < C::KPW; c++) su[c] = T(0);
-                            static_for<0, iy + jy + 1>([&](auto u_) {
-                                constexpr int u = decltype(u_)::value;
-                                T sv[C::KPW];
-#pragma unroll
-                                for (int c = 0; c < C::KPW; c++) sv[c] = T(0);
-                                static_for<0, iz + jz + 1>([&](auto v_) {
-                                    constexpr int v = decltype(v_)::value;
-                                    const T ez = sEu[2 * C::NE + e_offset<LJ>(iz, jz) + v];
-#pragma unroll
-                                    for (int c = 0; c < C::KPW; c++) sv[c] = fma(ez, Xh[c][herm_index(t, u, v)], sv[c]);
-                                });
-                                const T ey = sEu[C::NE + e_offset<LJ>(iy, jy) + u];
-#pragma unroll
-                                for (int c = 0; c < C::KPW; c++) su[c] = fma(ey, sv[c], su[c]);
-                            });
-                            const T ex = sEu[e_offset<LJ>(ix, jx) + t];
-#pragma unroll
-                            for (int c = 0; c < C::KPW; c++) sxv[c] = fma(ex, su[c], sxv[c]);
-                        });
-#pragma unroll
-                        for (int c = 0; c < C::KPW; c++)
-                            acc[ci * C::NJ + cj][c] = fma(pref, sxv[c], acc[ci * C::NJ + cj][c]);
-                    });
-                });
                 if constexpr (ONE) __syncwarp();
                 else __syncthreads();
             }
