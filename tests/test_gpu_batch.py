@@ -124,8 +124,8 @@ def _contracted_auxiliary_molecule():
 
 def test_contracted_auxiliary_every_variant_and_mixed():
     """Contracted, ragged auxiliary shells through every launch variant of the
-    fast kernels (one-warp and multi-warp CTAs) and through a mixed batch,
-    against the reference library."""
+    fast kernels (one-warp and multi-warp CTAs), FP64 and FP32, against the
+    reference library."""
     ref = oracle.reference()
     if ref is None:
         pytest.skip("reference library not built")
@@ -148,15 +148,26 @@ def test_contracted_auxiliary_every_variant_and_mixed():
         for k, v in saved.items():
             if v >= 0:
                 L.eip_tune_set(*k, v)
-    mix = bt.ThreeCenterBatch([m], [pd], [ad], precision="mixed", fp32_threshold=float("inf"))
-    mix.alloc_output()
-    mix.run()
-    mix.status()
-    err = np.max(np.abs(mix.dense(0) - want))
-    mix.close()
-    # every shell pair in FP32 (R, ket, bra): a loose bound that still catches
-    # any misplaced component or unit
-    assert 0.0 < err <= 1e-4 * max(1.0, float(np.max(np.abs(want)))), err
+    # every shell pair in FP32 (R, ket, bra), through every FP32 launch variant:
+    # a loose bound that still catches any misplaced component or unit
+    at = importlib.import_module("electron-integral-playground_b200.autotune")
+    saved32 = {k: L.eip_tune_get_fp32(*k) for k in saved}
+    try:
+        for v in at.FP32_VARIANTS:
+            for k in saved32:
+                if saved32[k] >= 0:
+                    assert L.eip_tune_set_fp32(*k, v) == 0
+            mix = bt.ThreeCenterBatch([m], [pd], [ad], precision="mixed", fp32_threshold=float("inf"))
+            mix.alloc_output()
+            mix.run()
+            mix.status()
+            err = np.max(np.abs(mix.dense(0) - want))
+            mix.close()
+            assert 0.0 < err <= 1e-4 * max(1.0, float(np.max(np.abs(want)))), (v, err)
+    finally:
+        for k, v in saved32.items():
+            if v >= 0:
+                L.eip_tune_set_fp32(*k, v)
 
 
 def _two_fragments():
