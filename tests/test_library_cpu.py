@@ -66,3 +66,35 @@ def test_empty_inputs_are_noops():
     assert L.three_center(0, 0, 0, dp(z), dp(z), dp(z), dp(z), ip(zi), ip(zi), 0, dp(z), dp(z), ip(zi), 1,
                           dp(out), 1, 1, True, 0.0) == 0
     assert L.overlap(0, 0, dp(z), dp(z), dp(z), ip(zi), ip(zi), 0, dp(out), 1, True) == 0
+
+
+def test_committed_tuning_table_is_valid():
+    """The autotuner's table for B200 names every fast class of the bench's
+    batch (orbital s-d pairs, auxiliary s-g) with a compiled variant, and the
+    library accepts each entry (the setters are host-side; no device)."""
+    if not lib_mod.LIB_PATH.exists():
+        pytest.skip("library not built")
+    at = importlib.import_module("electron-integral-playground_b200.autotune")
+    import json
+
+    data = json.loads(at.DEFAULT_CACHE.read_text())
+    classes = {f"{li},{lj},{lk}" for li in range(3) for lj in range(li, 3) for lk in range(5)}
+    assert set(data["variants"]) == classes
+    assert set(data["variants_fp32"]) == classes
+    assert all(v in range(at.N_VARIANTS) for v in data["variants"].values())
+    assert all(v in at.FP32_VARIANTS for v in data["variants_fp32"].values())
+    L = lib_mod.lib()
+    saved = {k: (L.eip_tune_get(*map(int, k.split(","))), L.eip_tune_get_fp32(*map(int, k.split(","))))
+             for k in classes}
+    try:
+        at.load()
+        for k in classes:
+            li, lj, lk = map(int, k.split(","))
+            assert L.eip_tune_get(li, lj, lk) == data["variants"][k]
+            assert L.eip_tune_get_fp32(li, lj, lk) == data["variants_fp32"][k]
+        assert L.eip_tune_set(0, 0, 0, at.N_VARIANTS) == 1  # out of range
+    finally:
+        for k, (v, v32) in saved.items():
+            li, lj, lk = map(int, k.split(","))
+            L.eip_tune_set(li, lj, lk, v)
+            L.eip_tune_set_fp32(li, lj, lk, v32)
