@@ -93,6 +93,7 @@ using namespace eip;
 
 struct eip_batch {
     int n_mol = 0;
+    int device = -1;       // device the batch was built on; its calls run there
     bool spherical = true;
     double omega = 0.0;
     int precision = 0;     // 0 FP64, 1 mixed (FP32 for bounded shell pairs)
@@ -144,6 +145,21 @@ struct eip_batch {
 };
 
 namespace {
+
+// Makes the batch's device current for one call and restores the caller's.
+struct OnDevice {
+    int saved = -1;
+    bool switched = false;
+    bool ok = true;
+    explicit OnDevice(const eip_batch* b) {
+        if (!b || b->device < 0 || cudaGetDevice(&saved) != cudaSuccess || saved == b->device) return;
+        ok = cudaSetDevice(b->device) == cudaSuccess;
+        switched = ok;
+    }
+    ~OnDevice() {
+        if (switched) cudaSetDevice(saved);
+    }
+};
 
 int fail(eip_batch* b, const char* what, cudaError_t e) {
     snprintf(b->err, sizeof b->err, "%s: %s", what, e == cudaSuccess ? "invalid" : cudaGetErrorString(e));
@@ -290,6 +306,9 @@ int eip_batch_add_charges(eip_batch* b, int mol, const double* position, int n_c
 int eip_batch_build(eip_batch* b) {
     if (!b || b->built) return 2;
     if (int rc = eip_init(-1)) return fail(b, eip_last_error(), cudaSuccess) ? rc : rc;
+    b->device = current_device();
+    if (b->device < 0) return fail(b, "no usable CUDA device", cudaErrorInvalidDevice);
+    if (int rc = ensure_device_tables()) return fail(b, "constant tables", (cudaError_t)rc);
     cudaError_t e;
     // ---- which classes exist
     std::map<std::pair<int, int>, int> pair_classes;
@@ -625,6 +644,8 @@ int eip_batch_bind_output(eip_batch* b, double* device_out) {
 
 int eip_batch_alloc_output(eip_batch* b) {
     if (!b || !b->built) return 2;
+    OnDevice on(b);
+    if (!on.ok) return fail(b, "cudaSetDevice (batch device)", cudaErrorInvalidDevice);
     double* p = nullptr;
     cudaError_t e = cudaMalloc((void**)&p, sizeof(double) * std::max<long long>(b->out_elems, 1));
     if (e != cudaSuccess) return fail(b, "output allocation", e);
@@ -720,6 +741,8 @@ static int capture(eip_batch* b, bool checksum) {
 
 int eip_batch_run(eip_batch* b, int checksum) {
     if (!b || !b->built || !b->d_out) return 2;
+    OnDevice on(b);
+    if (!on.ok) return fail(b, "cudaSetDevice (batch device)", cudaErrorInvalidDevice);
     if (!b->exec) {
         if (int rc = capture(b, checksum != 0)) return rc;
     }
@@ -730,6 +753,8 @@ int eip_batch_run(eip_batch* b, int checksum) {
 
 int eip_batch_run_class(eip_batch* b, int i_L, int j_L, int k_L) {
     if (!b || !b->built || !b->d_out) return 2;
+    OnDevice on(b);
+    if (!on.ok) return fail(b, "cudaSetDevice (batch device)", cudaErrorInvalidDevice);
     for (ClassPlan& pl : b->plans) {
         if (pl.li != i_L || pl.lj != j_L || pl.lk != k_L) continue;
         if (!pl.fast || (pl.total_items == 0 && pl.total_items32 == 0)) return 1;
@@ -836,6 +861,8 @@ int eip_batch_window_block(eip_batch* b, int mol, int i_L, int j_L, int k_L, lon
 
 int eip_batch_run_window(eip_batch* b, double* device_out, int checksum) {
     if (!b || !b->built || !b->win_planned || !device_out) return 2;
+    OnDevice on(b);
+    if (!on.ok) return fail(b, "cudaSetDevice (batch device)", cudaErrorInvalidDevice);
     cudaError_t e;
     const int nm = b->n_mol;
     const int n_side = b->n_streams;
@@ -993,6 +1020,7 @@ int eip_batch_copy_output(eip_batch* b, long long offset, long long count, doubl
 
 void eip_batch_destroy(eip_batch* b) {
     if (!b) return;
+    OnDevice on(b);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);

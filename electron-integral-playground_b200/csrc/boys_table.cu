@@ -2,15 +2,20 @@
 // copies of the spherical-harmonic / normalisation coefficients.
 #include <math.h>
 
+#include <mutex>
+
 #include "eip_common.cuh"
 #include "eip_internal.h"
 
 namespace eip {
 
 __device__ double g_boys_table[kBoysGrid * kBoysOrders];
-static const double* g_boys_table_address = nullptr;
 
-const double* boys_table_device() { return g_boys_table_address; }
+namespace {
+// Device address of g_boys_table per device (nullptr: tables not uploaded yet).
+std::atomic<const double*> g_boys_address[kMaxDevices];
+std::mutex g_tables_mu;
+}  // namespace
 
 // F_m(T0) on the grid: F_M(T0) = e^-T0 sum_k (2 T0)^k / ((2M+1)(2M+3)...(2M+2k+1))
 // (all terms positive: no cancellation), in long double, then the downward
@@ -33,7 +38,12 @@ static void build_boys_table(double* out) {
     }
 }
 
-int upload_constant_tables() {
+int ensure_device_tables() {
+    const int dev = current_device();
+    if (dev < 0) return (int)cudaErrorInvalidDevice;
+    if (g_boys_address[dev].load(std::memory_order_acquire)) return 0;
+    std::lock_guard<std::mutex> lock(g_tables_mu);
+    if (g_boys_address[dev].load(std::memory_order_acquire)) return 0;
     static double host_table[kBoysGrid * kBoysOrders];
     static bool built = false;
     if (!built) {
@@ -44,8 +54,18 @@ int upload_constant_tables() {
     void* addr = nullptr;
     if (e == cudaSuccess) e = cudaGetSymbolAddress(&addr, g_boys_table);
     if (e != cudaSuccess) return (int)e;
-    g_boys_table_address = static_cast<const double*>(addr);
-    return upload_generic_tables();
+    if (int rc = upload_generic_tables()) return rc;
+    // published last: a non-null address means every table of the device is in place
+    g_boys_address[dev].store(static_cast<const double*>(addr), std::memory_order_release);
+    return 0;
+}
+
+const double* boys_table_device() {
+    const int dev = current_device();
+    if (dev < 0) return nullptr;
+    const double* t = g_boys_address[dev].load(std::memory_order_acquire);
+    if (t) return t;
+    return ensure_device_tables() == 0 ? g_boys_address[dev].load(std::memory_order_acquire) : nullptr;
 }
 
 // Evaluate F_0..F_L on the device for a list of T (tests the device Boys).
@@ -60,7 +80,9 @@ __global__ void boys_probe_kernel(const double* __restrict__ table, int L, const
 int launch_boys_probe(int L, const double* dT, int n, double* dout, cudaStream_t s) {
     if (L < 0 || L > kMaxBoysM) return 1;
     if (n <= 0) return 0;
-    boys_probe_kernel<<<(n + 127) / 128, 128, 0, s>>>(g_boys_table_address, L, dT, n, dout);
+    const double* table = boys_table_device();
+    if (!table) return 2;
+    boys_probe_kernel<<<(n + 127) / 128, 128, 0, s>>>(table, L, dT, n, dout);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 

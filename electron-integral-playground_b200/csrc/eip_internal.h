@@ -4,15 +4,36 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include <atomic>
+
 namespace eip {
 
 struct BraTable;
 struct KetTable;
 struct BatchMap;
 
-int upload_constant_tables();
+// Per-device state.  Every device this process uses gets its own copy of the
+// constant tables (module data is per device), its own Boys-grid address and
+// its own launch attributes; everything is keyed by the device current on the
+// calling thread and set up once, under a lock, by the first use on it.
+constexpr int kMaxDevices = 64;
+// Current device of the calling thread, or -1 (no device / out of range).
+int current_device();
+// Uploads the constant tables to the current device once (thread-safe);
+// returns 0 or a cudaError_t value.
+int ensure_device_tables();
 int upload_generic_tables();
+// Device address of the Boys grid on the current device (sets the device up
+// on first use); nullptr if that failed.
 const double* boys_table_device();
+// Occupancy-sized persistent grid of one kernel on the current device: the
+// kernel's dynamic shared-memory limit is raised to smem_bytes and the
+// per-device result is cached in *cache (an array of kMaxDevices entries,
+// 0 = not yet computed).  Returns the grid size, or 0 on failure.
+int persistent_grid(const void* kernel, int threads, size_t smem_bytes, std::atomic<int>* cache);
+// Records the calling thread's last error (eip_last_error) and prints it:
+// "<what>: <CUDA error string>", or "<what>" alone for cudaSuccess.
+void set_error(const char* what, cudaError_t e);
 int launch_boys_probe(int L, const double* dT, int n, double* dout, cudaStream_t s);
 
 bool fast3c_supported(int li, int lj, int lk);

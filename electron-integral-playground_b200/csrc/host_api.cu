@@ -29,14 +29,16 @@
 #include "../../include/eip_b200.h"
 
 namespace eip {
-namespace {
 
 thread_local char g_last_error[512] = "";
 
 void set_error(const char* what, cudaError_t e) {
-    snprintf(g_last_error, sizeof g_last_error, "%s: %s", what, e == cudaSuccess ? "failed" : cudaGetErrorString(e));
+    if (e == cudaSuccess) snprintf(g_last_error, sizeof g_last_error, "%s", what);
+    else snprintf(g_last_error, sizeof g_last_error, "%s: %s", what, cudaGetErrorString(e));
     fprintf(stderr, "[eip] %s\n", g_last_error);
 }
+
+namespace {
 
 struct DeviceBuffer {
     void* ptr = nullptr;
@@ -84,12 +86,40 @@ Context& ctx() {
     return c;
 }
 
-int ensure_context_locked(Context& c) {
-    if (c.device >= 0) return 0;
+// The reference-ABI calls run on the library context's device (the one
+// current at eip_init or at the first call), whatever device the calling
+// thread has current; the caller's device is restored on return.
+struct DeviceGuard {
+    int saved = -1;
+    bool switched = false;
+    cudaError_t enter(int dev) {
+        cudaError_t e = cudaGetDevice(&saved);
+        if (e != cudaSuccess) return e;
+        if (saved == dev) return cudaSuccess;
+        e = cudaSetDevice(dev);
+        switched = e == cudaSuccess;
+        return e;
+    }
+    ~DeviceGuard() {
+        if (switched) cudaSetDevice(saved);
+    }
+};
+
+int ensure_context_locked(Context& c, DeviceGuard* guard = nullptr) {
+    if (c.device >= 0) {
+        if (guard) {
+            cudaError_t e = guard->enter(c.device);
+            if (e != cudaSuccess) {
+                set_error("cudaSetDevice (library context device)", e);
+                return 2;
+            }
+        }
+        return 0;
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        set_error("no CUDA device", e);
+    if (e != cudaSuccess || dev >= kMaxDevices) {
+        set_error("no usable CUDA device", e);
         return 2;
     }
     e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
@@ -101,7 +131,7 @@ int ensure_context_locked(Context& c) {
         set_error("cudaEventCreate", cudaGetLastError());
         return 2;
     }
-    if (int rc = upload_constant_tables()) {
+    if (int rc = ensure_device_tables()) {
         set_error("constant table upload", (cudaError_t)rc);
         return 2;
     }
@@ -397,7 +427,8 @@ int eip_tune_get_fp32(int i_L, int j_L, int k_L) { return fast3c_variant_fp32(i_
 int eip_boys(int L, const double* T, int n, double* F) {
     Context& c = ctx();
     std::lock_guard<std::mutex> lock(c.mu);
-    if (int rc = ensure_context_locked(c)) return rc;
+    DeviceGuard guard;
+    if (int rc = ensure_context_locked(c, &guard)) return rc;
     if (L < 0 || L > kMaxBoysM) return 1;
     if (n <= 0) return 0;
     const size_t out_bytes = sizeof(double) * (size_t)n * (L + 1);
@@ -430,7 +461,8 @@ int three_center(const int i_L, const int j_L, const int k_L, const double* pair
     if (n_pair_ij <= 0 || n_aux_primitive_k <= 0) return 0;
     Context& c = ctx();
     std::lock_guard<std::mutex> lock(c.mu);
-    if (int rc = ensure_context_locked(c)) return rc;
+    DeviceGuard guard;
+    if (int rc = ensure_context_locked(c, &guard)) return rc;
     Staged st;
     PairGroups bg, kg;
     BraInput bi{0, pair_P_p, pair_A_a, pair_B_b, pair_coefficient, pair_i_ao_start, pair_j_ao_start, n_pair_ij};
@@ -469,7 +501,8 @@ int two_center(const int i_L, const int j_L, const double* aux_A_a, const double
     if (n_aux_primitive_i <= 0 || n_aux_primitive_j <= 0) return 0;
     Context& c = ctx();
     std::lock_guard<std::mutex> lock(c.mu);
-    if (int rc = ensure_context_locked(c)) return rc;
+    DeviceGuard guard;
+    if (int rc = ensure_context_locked(c, &guard)) return rc;
     Staged st;
     PairGroups bg, kg;
     BraInput bi{1, nullptr, aux_A_a, nullptr, aux_i_coefficient, aux_i_aux_start, nullptr, n_aux_primitive_i};
@@ -509,7 +542,8 @@ int nuclear_attraction(const int i_L, const int j_L, const double* pair_P_p, con
     if (n_pair <= 0 || n_charge <= 0) return 0;
     Context& c = ctx();
     std::lock_guard<std::mutex> lock(c.mu);
-    if (int rc = ensure_context_locked(c)) return rc;
+    DeviceGuard guard;
+    if (int rc = ensure_context_locked(c, &guard)) return rc;
     Staged st;
     PairGroups bg, kg;
     BraInput bi{0, pair_P_p, pair_A_a, pair_B_b, pair_coefficient, pair_i_ao_start, pair_j_ao_start, n_pair};
@@ -545,7 +579,8 @@ int overlap(const int i_L, const int j_L, const double* pair_A_a, const double* 
     if (n_pair <= 0) return 0;
     Context& c = ctx();
     std::lock_guard<std::mutex> lock(c.mu);
-    if (int rc = ensure_context_locked(c)) return rc;
+    DeviceGuard guard;
+    if (int rc = ensure_context_locked(c, &guard)) return rc;
     // The overlap entry carries no P_p: rebuild (P, p) rows from A and B.
     std::vector<double> P(4 * (size_t)n_pair);
     for (int k = 0; k < n_pair; k++) {

@@ -1,6 +1,7 @@
-// Dispatcher of the fast (mu nu|P) kernels: one translation unit per (l_i, l_j)
-// and tuning variant (k3c_fast_IJ_vV.cu) so the instances compile in parallel;
-// the variant of each class comes from the tuning table (eip_tune_set).
+// Dispatcher of the fast (mu nu|P) kernels: one compiled instance per (l_i, l_j)
+// pair class, tuning variant and type (k3c_fast_inst.cu, built once per
+// instance by the Makefile) so the instances compile in parallel; the variant
+// of each class comes from the tuning table (eip_tune_set).
 #include "eip_common.cuh"
 #include "eip_internal.h"
 
@@ -17,10 +18,7 @@ namespace eip {
 #define EIP_DECL(I, J)                                                                                      \
     EIP_DECL_V(I, J, 0) EIP_DECL_V(I, J, 1) EIP_DECL_V(I, J, 2) EIP_DECL_V(I, J, 3) EIP_DECL_V(I, J, 4)     \
     EIP_DECL_V(I, J, 5)                                                                                     \
-    int launch_fast3c_##I##J##_f32(int lk, const double* boys_table, const BraTable& bra, const KetTable& ket, \
-                                   const BatchMap& map, int total_items, double omega, double* out,         \
-                                   int* counter, cudaStream_t s);                                           \
-    EIP_DECL_F(I, J, 2) EIP_DECL_F(I, J, 3) EIP_DECL_F(I, J, 4)                                              \
+    EIP_DECL_F(I, J, 0) EIP_DECL_F(I, J, 2) EIP_DECL_F(I, J, 3) EIP_DECL_F(I, J, 4)                          \
     int launch_e_table_##I##J(const BraTable& bra, double* prim_E, cudaStream_t s);
 EIP_DECL(0, 0) EIP_DECL(0, 1) EIP_DECL(1, 1) EIP_DECL(0, 2) EIP_DECL(1, 2) EIP_DECL(2, 2) EIP_DECL(0, 3) EIP_DECL(0, 4)
 #undef EIP_DECL
@@ -71,6 +69,7 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
                   int total_items, double omega, double* out, int* counter, cudaStream_t s, bool fp32) {
     if (!fast3c_supported(li, lj, lk)) return 1;
     const double* t = boys_table_device();
+    if (!t) return 2;
     const int v = fp32 ? -1 - g_variant32[li][lj][lk] : g_variant[li][lj][lk];
 #define EIP_GO_V(I, J, V) return launch_fast3c_##I##J##_v##V(lk, t, bra, ket, map, total_items, omega, out, counter, s)
 #define EIP_GO(I, J)                                                                                          \
@@ -80,7 +79,7 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
         case 3: EIP_GO_V(I, J, 3);                                                                            \
         case 4: EIP_GO_V(I, J, 4);                                                                            \
         case 5: EIP_GO_V(I, J, 5);                                                                            \
-        case -1: return launch_fast3c_##I##J##_f32(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
+        case -1: return launch_fast3c_##I##J##_f32_v0(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
         case -3: return launch_fast3c_##I##J##_f32_v2(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
         case -4: return launch_fast3c_##I##J##_f32_v3(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
         case -5: return launch_fast3c_##I##J##_f32_v4(lk, t, bra, ket, map, total_items, omega, out, counter, s); \

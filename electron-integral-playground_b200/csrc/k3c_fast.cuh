@@ -625,27 +625,19 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
     }
 }
 
-// Occupancy-sized persistent grid for one class.
+// Occupancy-sized persistent grid for one class (per device: the shared-memory
+// attribute and the occupancy are set up on each device's first launch).
 template <int LI, int LJ, int LK, int V, typename T, bool POINT = false>
 static int launch_one(const double* boys_table, const BraTable& bra, const KetTable& ket, const BatchMap& map,
                       int total_items, double omega, double* out, int* counter, cudaStream_t s) {
     using C = Fast3c<LI, LJ, LK, V>;
     if (total_items <= 0) return 0;
     constexpr size_t smem = C::template smem_bytes<T>();
-    static int max_blocks = 0;
-    if (max_blocks == 0) {
-        int per_sm = 0, dev = 0, sms = 0;
-        if (cudaFuncSetAttribute(k3c_fast<LI, LJ, LK, V, T, POINT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess)
-            return 2;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3c_fast<LI, LJ, LK, V, T, POINT>, C::THREADS,
-                                                          smem) != cudaSuccess)
-            return 2;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        max_blocks = (per_sm < 1 ? 1 : per_sm) * sms;
-    }
-    const int blocks = total_items < max_blocks ? total_items : max_blocks;
+    static std::atomic<int> max_blocks[kMaxDevices];
+    const int grid = persistent_grid(reinterpret_cast<const void*>(k3c_fast<LI, LJ, LK, V, T, POINT>), C::THREADS,
+                                     smem, max_blocks);
+    if (grid <= 0) return 2;
+    const int blocks = total_items < grid ? total_items : grid;
     k3c_fast<LI, LJ, LK, V, T, POINT><<<blocks, C::THREADS, smem, s>>>(boys_table, bra, ket, map, omega, out,
                                                                        counter, total_items);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;

@@ -9,6 +9,7 @@ namespace eip {
 int launch_fast_point(int li, int lj, const BraTable& bra, const KetTable& ket, const BatchMap& map,
                       int total_items, double omega, double* out, int* counter, cudaStream_t s) {
     const double* t = boys_table_device();
+    if (!t) return 2;
 #define EIP_P(I, J) \
     return launch_one<I, J, 0, (I + J >= 3 ? 3 : 0), double, true>(t, bra, ket, map, total_items, omega, out, counter, s)
     switch (li * 10 + lj) {

@@ -19,6 +19,8 @@
 // transform_kernel: raw Cartesian blocks -> spherical (real solid harmonics)
 // or per-component-normalised Cartesian output, written in the packed layout
 //   out[((bra * n_io * n_jo + I * n_jo + J) * n_ko + K) * n_ket + ket].
+#include <algorithm>
+
 #include "eip_common.cuh"
 #include "eip_internal.h"
 
@@ -372,22 +374,33 @@ int generic_kc_chunk(int li, int lj, int lk) {
     return chunk;
 }
 
+// Largest dynamic shared memory raw_kernel takes over every class the C ABI
+// accepts (orbital l <= 6, auxiliary l <= 9; the two-centre bra up to l = 9).
+static size_t generic_max_smem() {
+    size_t m = 0;
+    for (int li = 0; li <= kMaxAuxL; li++)
+        for (int lj = 0; lj <= kMaxOrbitalL; lj++)
+            for (int lk = 0; lk <= kMaxAuxL; lk++)
+                if (li + lj + lk <= kMaxBoysM) m = std::max(m, generic_smem_bytes(li, lj, lk, generic_kc_chunk(li, lj, lk)));
+    return m;
+}
+
 int launch_generic_raw(int mode, int li, int lj, int lk, const BraTable& bra, const KetTable& ket, double omega,
                        int skip_lower, double* raw, cudaStream_t s) {
     if (bra.n_group == 0 || ket.n_group == 0) return 0;
     const int chunk = generic_kc_chunk(li, lj, lk);
     const int n_chunks = (ncart(lk) + chunk - 1) / chunk;
     const size_t smem = generic_smem_bytes(li, lj, lk, chunk);
-    static size_t configured = 0;
-    if (smem > configured) {
-        if (cudaFuncSetAttribute(raw_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return 2;
-        configured = smem;
-    }
+    // the shared-memory limit is raised once per device, to the largest class's
+    // need (persistent_grid caches per device and serialises the set-up)
+    static std::atomic<int> configured[kMaxDevices];
+    if (persistent_grid(reinterpret_cast<const void*>(raw_kernel), kGenThreads, generic_max_smem(), configured) <= 0)
+        return 2;
+    const double* table = boys_table_device();
+    if (!table) return 2;
     if (ket.n_group > 65535) return 3;
     dim3 grid(bra.n_group, ket.n_group, n_chunks);
-    raw_kernel<<<grid, kGenThreads, smem, s>>>(boys_table_device(), mode, li, lj, lk, chunk, bra, ket, omega,
-                                               skip_lower, raw);
+    raw_kernel<<<grid, kGenThreads, smem, s>>>(table, mode, li, lj, lk, chunk, bra, ket, omega, skip_lower, raw);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 

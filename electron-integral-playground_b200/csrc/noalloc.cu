@@ -26,11 +26,17 @@
 // Set-up: the first call on each device (with that device current) looks up
 // the array's device address with cudaGetSymbolAddress and uploads the
 // library's constant tables (Boys grid, spherical coefficients) with
-// cudaMemcpyToSymbol; make that first call before any stream capture.  Later
-// calls only launch kernels on the given stream, asynchronously.
+// cudaMemcpyToSymbol, once per device under a lock (several host threads may
+// make first calls at once); make that first call before any stream capture.
+// Later calls only launch kernels on the given stream, asynchronously.
+//
+// eip_three_center_noalloc_check() computes a call's working-memory need on
+// the host (no CUDA call), so a caller can split its work before calling.
 #include <stdio.h>
 
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 
 #include "eip_common.cuh"
 #include "eip_internal.h"
@@ -40,17 +46,72 @@ namespace eip {
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
-constexpr int kMaxDevices = 64;
+constexpr int kNoAllocMaxAuxPrimitives = 65535;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-struct DeviceSetup {
-    bool ready = false;
-    unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch
-};
-DeviceSetup g_setup[kMaxDevices];
+// Device address of g_noalloc_scratch per device; null until that device's set-up.
+std::atomic<unsigned char*> g_scratch_address[kMaxDevices];
+std::mutex g_setup_mu;
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Byte offsets of one call's arrays in the scratch array.
+struct ScratchLayout {
+    size_t bbeg, bao, bab, bp, bpa, kbeg, kst, kc, kco, raw, pk, total;
+};
+
+ScratchLayout scratch_layout(int i_L, int j_L, int k_L, size_t np, size_t na, bool spherical) {
+    const size_t ni = spherical ? nsph(i_L) : ncart(i_L), nj = spherical ? nsph(j_L) : ncart(j_L),
+                 nk = spherical ? nsph(k_L) : ncart(k_L);
+    ScratchLayout l{};
+    size_t off = 0;
+    l.bbeg = off; off += align256(sizeof(int) * (np + 1));
+    l.bao = off; off += align256(sizeof(int2) * np);
+    l.bab = off; off += align256(sizeof(double4) * np);
+    l.bp = off; off += align256(sizeof(double4) * np);
+    l.bpa = off; off += align256(sizeof(double4) * np);
+    l.kbeg = off; off += align256(sizeof(int) * (na + 1));
+    l.kst = off; off += align256(sizeof(int) * na);
+    l.kc = off; off += align256(sizeof(double4) * na);
+    l.kco = off; off += align256(sizeof(double) * na);
+    l.raw = off; off += align256(sizeof(double) * np * na * ncart(i_L) * ncart(j_L) * ncart(k_L));
+    l.pk = off; off += align256(sizeof(double) * np * na * ni * nj * nk);
+    l.total = off;
+    return l;
+}
+
+bool class_supported(int i_L, int j_L, int k_L) {
+    return i_L >= 0 && j_L >= 0 && k_L >= 0 && i_L <= j_L && j_L <= kMaxOrbitalL && k_L <= kMaxAuxL;
+}
+
+// Device address of the scratch array on the current device, setting the
+// device up (address lookup, constant tables) on its first call; null on failure.
+unsigned char* scratch_on_current_device() {
+    const int dev = current_device();
+    if (dev < 0) {
+        set_error("eip_three_center_noalloc: no usable CUDA device", cudaGetLastError());
+        return nullptr;
+    }
+    unsigned char* p = g_scratch_address[dev].load(std::memory_order_acquire);
+    if (p) return p;
+    std::lock_guard<std::mutex> lock(g_setup_mu);
+    p = g_scratch_address[dev].load(std::memory_order_acquire);
+    if (p) return p;
+    void* addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess || addr == nullptr) {
+        set_error("eip_three_center_noalloc: cudaGetSymbolAddress", e);
+        return nullptr;
+    }
+    if (int rc = ensure_device_tables()) {
+        set_error("eip_three_center_noalloc: constant table upload", (cudaError_t)rc);
+        return nullptr;
+    }
+    p = static_cast<unsigned char*>(addr);
+    g_scratch_address[dev].store(p, std::memory_order_release);
+    return p;
+}
 
 // Reference-format device arrays -> the generic kernel's tables, one group per
 // primitive pair and per auxiliary primitive (no grouping: nothing to sort).
@@ -110,6 +171,19 @@ __global__ void noalloc_scatter_kernel(const double* __restrict__ packed, const 
 
 using namespace eip;
 
+extern "C" size_t eip_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
+
+extern "C" int eip_three_center_noalloc_check(const int i_L, const int j_L, const int k_L, const int n_pair_ij,
+                                              const int n_aux_primitive_k, const bool spherical,
+                                              size_t* bytes_needed) {
+    if (bytes_needed) *bytes_needed = 0;
+    if (!class_supported(i_L, j_L, k_L)) return 1;
+    if (n_pair_ij <= 0 || n_aux_primitive_k <= 0) return 0;
+    const ScratchLayout l = scratch_layout(i_L, j_L, k_L, (size_t)n_pair_ij, (size_t)n_aux_primitive_k, spherical);
+    if (bytes_needed) *bytes_needed = l.total;
+    return l.total > kNoAllocScratchBytes || n_aux_primitive_k > kNoAllocMaxAuxPrimitives ? 4 : 0;
+}
+
 extern "C" int eip_three_center_noalloc(const int i_L, const int j_L, const int k_L, const double* pair_P_p,
                                         const double* pair_A_a, const double* pair_B_b,
                                         const double* pair_coefficient, const int* pair_i_ao_start,
@@ -118,79 +192,51 @@ extern "C" int eip_three_center_noalloc(const int i_L, const int j_L, const int 
                                         const int n_aux_primitive_k, double* J3c_matrix, const int n_ao,
                                         const int n_aux, const bool spherical, const double omega, void* stream) {
     (void)n_aux;
-    if (i_L < 0 || j_L < 0 || k_L < 0 || i_L > j_L || j_L > kMaxOrbitalL || k_L > kMaxAuxL) {
+    size_t need = 0;
+    const int fit = eip_three_center_noalloc_check(i_L, j_L, k_L, n_pair_ij, n_aux_primitive_k, spherical, &need);
+    if (fit == 1) {
         printf("%s function does not support angular i_L = %d, j_L = %d, k_L = %d\n", __func__, i_L, j_L, k_L);
         fflush(stdout);
         return 1;
     }
     if (n_pair_ij <= 0 || n_aux_primitive_k <= 0) return 0;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-        fprintf(stderr, "[eip] eip_three_center_noalloc: no usable CUDA device (%s)\n", cudaGetErrorString(e));
-        return 2;
+    if (fit == 4) {
+        char msg[384];
+        snprintf(msg, sizeof msg,
+                 "eip_three_center_noalloc: class (%d%d|%d) with %d primitive pairs x %d auxiliary primitives needs "
+                 "%zu bytes of working memory; the fixed limit is %zu bytes and %d auxiliary primitives: split the "
+                 "call or use three_center()",
+                 i_L, j_L, k_L, n_pair_ij, n_aux_primitive_k, need, kNoAllocScratchBytes, kNoAllocMaxAuxPrimitives);
+        set_error(msg, cudaSuccess);
+        return 4;
     }
-    DeviceSetup& S = g_setup[dev];
-    if (!S.ready) {
-        void* addr = nullptr;
-        e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
-        if (e != cudaSuccess || addr == nullptr) {
-            fprintf(stderr, "[eip] eip_three_center_noalloc: cudaGetSymbolAddress failed (%s)\n",
-                    cudaGetErrorString(e));
-            return 2;
-        }
-        if (int rc = upload_constant_tables()) {
-            fprintf(stderr, "[eip] eip_three_center_noalloc: constant table upload failed (%d)\n", rc);
-            return 2;
-        }
-        S.scratch = static_cast<unsigned char*>(addr);
-        S.ready = true;
-    }
-    // Scratch layout of this call.
+    unsigned char* s = scratch_on_current_device();
+    if (!s) return 2;
     const size_t np = (size_t)n_pair_ij, na = (size_t)n_aux_primitive_k;
     const int ni = spherical ? nsph(i_L) : ncart(i_L), nj = spherical ? nsph(j_L) : ncart(j_L),
               nk = spherical ? nsph(k_L) : ncart(k_L);
-    size_t off = 0;
-    const size_t o_bbeg = off; off += align256(sizeof(int) * (np + 1));
-    const size_t o_bao = off; off += align256(sizeof(int2) * np);
-    const size_t o_bab = off; off += align256(sizeof(double4) * np);
-    const size_t o_bp = off; off += align256(sizeof(double4) * np);
-    const size_t o_bpa = off; off += align256(sizeof(double4) * np);
-    const size_t o_kbeg = off; off += align256(sizeof(int) * (na + 1));
-    const size_t o_kst = off; off += align256(sizeof(int) * na);
-    const size_t o_kc = off; off += align256(sizeof(double4) * na);
-    const size_t o_kco = off; off += align256(sizeof(double) * na);
-    const size_t o_raw = off; off += align256(sizeof(double) * np * na * ncart(i_L) * ncart(j_L) * ncart(k_L));
-    const size_t o_pk = off; off += align256(sizeof(double) * np * na * ni * nj * nk);
-    if (off > kNoAllocScratchBytes || na > 65535) {
-        fprintf(stderr,
-                "[eip] eip_three_center_noalloc: class (%d%d|%d) with %d primitive pairs x %d auxiliary primitives "
-                "needs %zu bytes of working memory; the fixed limit is %zu bytes (and <= 65535 auxiliary "
-                "primitives): split the call or use three_center()\n",
-                i_L, j_L, k_L, n_pair_ij, n_aux_primitive_k, off, kNoAllocScratchBytes);
-        return 4;
-    }
-    unsigned char* s = S.scratch;
+    const ScratchLayout l = scratch_layout(i_L, j_L, k_L, np, na, spherical);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int nmax = (int)std::max(np, na) + 1;
     noalloc_tables_kernel<<<(nmax + 127) / 128, 128, 0, st>>>(
         pair_P_p, pair_A_a, pair_B_b, pair_coefficient, pair_i_ao_start, pair_j_ao_start, n_pair_ij, aux_A_a,
-        aux_coefficient, aux_i_aux_start, n_aux_primitive_k, reinterpret_cast<int*>(s + o_bbeg),
-        reinterpret_cast<int2*>(s + o_bao), reinterpret_cast<double4*>(s + o_bab),
-        reinterpret_cast<double4*>(s + o_bp), reinterpret_cast<double4*>(s + o_bpa),
-        reinterpret_cast<int*>(s + o_kbeg), reinterpret_cast<int*>(s + o_kst), reinterpret_cast<double4*>(s + o_kc),
-        reinterpret_cast<double*>(s + o_kco));
-    if ((e = cudaGetLastError()) != cudaSuccess) {
-        fprintf(stderr, "[eip] eip_three_center_noalloc: launch failed (%s)\n", cudaGetErrorString(e));
+        aux_coefficient, aux_i_aux_start, n_aux_primitive_k, reinterpret_cast<int*>(s + l.bbeg),
+        reinterpret_cast<int2*>(s + l.bao), reinterpret_cast<double4*>(s + l.bab),
+        reinterpret_cast<double4*>(s + l.bp), reinterpret_cast<double4*>(s + l.bpa),
+        reinterpret_cast<int*>(s + l.kbeg), reinterpret_cast<int*>(s + l.kst), reinterpret_cast<double4*>(s + l.kc),
+        reinterpret_cast<double*>(s + l.kco));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("eip_three_center_noalloc: table kernel launch", e);
         return 2;
     }
-    BraTable bra{n_pair_ij, reinterpret_cast<int*>(s + o_bbeg), reinterpret_cast<int2*>(s + o_bao),
-                 reinterpret_cast<double4*>(s + o_bab), reinterpret_cast<double4*>(s + o_bp),
-                 reinterpret_cast<double4*>(s + o_bpa), nullptr};
-    KetTable ket{n_aux_primitive_k, reinterpret_cast<int*>(s + o_kbeg), reinterpret_cast<int*>(s + o_kst),
-                 reinterpret_cast<double4*>(s + o_kc), reinterpret_cast<double*>(s + o_kco)};
-    double* raw = reinterpret_cast<double*>(s + o_raw);
-    double* packed = reinterpret_cast<double*>(s + o_pk);
+    BraTable bra{n_pair_ij, reinterpret_cast<int*>(s + l.bbeg), reinterpret_cast<int2*>(s + l.bao),
+                 reinterpret_cast<double4*>(s + l.bab), reinterpret_cast<double4*>(s + l.bp),
+                 reinterpret_cast<double4*>(s + l.bpa), nullptr};
+    KetTable ket{n_aux_primitive_k, reinterpret_cast<int*>(s + l.kbeg), reinterpret_cast<int*>(s + l.kst),
+                 reinterpret_cast<double4*>(s + l.kc), reinterpret_cast<double*>(s + l.kco)};
+    double* raw = reinterpret_cast<double*>(s + l.raw);
+    double* packed = reinterpret_cast<double*>(s + l.pk);
     int rc = launch_generic_raw(0, i_L, j_L, k_L, bra, ket, omega, 0, raw, st);
     if (rc == 0) rc = launch_transform(i_L, j_L, k_L, spherical, n_pair_ij, n_aux_primitive_k, raw, packed, st);
     if (rc == 0) {
@@ -202,7 +248,7 @@ extern "C" int eip_three_center_noalloc(const int i_L, const int j_L, const int 
         rc = cudaGetLastError() == cudaSuccess ? 0 : 2;
     }
     if (rc != 0) {
-        fprintf(stderr, "[eip] eip_three_center_noalloc: kernel launch failed\n");
+        set_error("eip_three_center_noalloc: kernel launch", cudaGetLastError());
         return 2;
     }
     return 0;

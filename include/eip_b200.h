@@ -66,7 +66,11 @@ int overlap(const int i_L, const int j_L, const double* pair_A_a, const double* 
 /* ---- extensions (no counterpart in the reference) ------------------------ */
 
 /* Select the device (or -1: the current one) and create the library's stream
- * and device tables.  Optional: every entry point initialises lazily. */
+ * and device tables.  Optional: every entry point initialises lazily.  The
+ * reference-ABI entry points run on this device (the first one initialised)
+ * whatever device the calling thread has current, and restore the caller's
+ * device; a batch runs on the device it was built on.  Each device that is
+ * used gets its own constant tables and launch set-up. */
 int eip_init(int device);
 
 /* Description of the last CUDA failure of the calling thread ("" if none). */
@@ -100,14 +104,15 @@ int eip_boys(int L, const double* T, int n, double* F);
  * Every pointer is a DEVICE pointer; J3c_matrix[n_aux][n_ao][n_ao] is
  * accumulated (+=) asynchronously on `stream` (a cudaStream_t, 0 = default).
  * Nothing is allocated: working memory is one fixed 16 MiB device array per
- * GPU, held from module load until exit.  Limit: a call needing more of it
- * (roughly n_pair_ij x n_aux_primitive_k primitive triplets times the class's
- * Cartesian plus output block) returns 4 with a message on stderr and launches
- * nothing; at most 65535 auxiliary primitives.  All calls share the array:
- * calls whose kernels overlap on the GPU race, so order them (one stream).
- * The first call on each device (with it current) looks up the array's address
- * and uploads the constant tables; make it before any stream capture.
- * Returns 0, 1 (unsupported class), 2 (CUDA failure) or 4 (too large). */
+ * GPU (eip_noalloc_scratch_bytes()), held from module load until exit.  Limit:
+ * a call needing more of it, or more than 65535 auxiliary primitives, returns
+ * 4 and launches nothing; eip_three_center_noalloc_check() tells beforehand,
+ * on the host, without any CUDA call.  All calls share the array: calls whose
+ * kernels overlap on the GPU race, so order them (one stream).  The first call
+ * on each device (with it current) looks up the array's address and uploads
+ * the constant tables, once per device under a lock; make it before any stream
+ * capture.  Returns 0, 1 (unsupported class), 2 (CUDA failure) or 4 (too
+ * large); for 2 and 4, eip_last_error() describes the failure. */
 int eip_three_center_noalloc(const int i_L, const int j_L, const int k_L,
                              const double* pair_P_p, const double* pair_A_a, const double* pair_B_b,
                              const double* pair_coefficient, const int* pair_i_ao_start,
@@ -115,6 +120,13 @@ int eip_three_center_noalloc(const int i_L, const int j_L, const int k_L,
                              const double* aux_coefficient, const int* aux_i_aux_start,
                              const int n_aux_primitive_k, double* J3c_matrix, const int n_ao, const int n_aux,
                              const bool spherical, const double omega, void* stream);
+/* Host-side admission test of eip_three_center_noalloc for one class and size:
+ * 0 = fits (*bytes_needed = its working memory, 0 for an empty call),
+ * 1 = unsupported class, 4 = too large (*bytes_needed = what it would need). */
+int eip_three_center_noalloc_check(const int i_L, const int j_L, const int k_L, const int n_pair_ij,
+                                   const int n_aux_primitive_k, const bool spherical, size_t* bytes_needed);
+/* Size of the fixed working array of eip_three_center_noalloc, in bytes. */
+size_t eip_noalloc_scratch_bytes(void);
 
 /* ---- screened pair tables built on the device (no counterpart in the C ABI:
  * replaces the reference front end's Python form_pair_data,

@@ -3,7 +3,9 @@
 Run in a container that has the reference checkout and its library built by
 ``make -C oracle ref``::
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference <reference checkout>]
+
+(default: $EIP_REFERENCE_ROOT).
 
 For every integral test of the reference (electron_integral_playground/
 molecular_integral/tests/test_*_integral.py) the script runs the test
@@ -39,8 +41,10 @@ MAX_FULL = 20000  # store full outputs up to this many elements, else subsample
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("EIP_REFERENCE_ROOT"))
     args = ap.parse_args()
+    if not args.reference or not (pathlib.Path(args.reference) / "electron_integral_playground").is_dir():
+        sys.exit("make_golden: give the reference checkout with --reference or EIP_REFERENCE_ROOT")
     ref_lib_dir = REPO / "oracle" / "_ref"
     if str(ref_lib_dir) not in os.environ.get("LD_LIBRARY_PATH", ""):
         # The reference wrappers dlopen("libmolecular_integral.so") at import.

@@ -17,7 +17,8 @@ lib_mod = importlib.import_module("electron-integral-playground_b200._lib")
 def declared_symbols():
     text = (REPO / "include" / "eip_b200.h").read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(?:int|void|const char\s*\*|unsigned long long)\s+(\w+)\s*\(", text)))
+    ret = r"(?:int|void|size_t|float|double\s*\*|long long|void\s*\*|const char\s*\*|unsigned long long|eip_\w+\s*\*)"
+    return sorted(set(re.findall(r"\b" + ret + r"\s*(\w+)\s*\(", text)))
 
 
 def test_header_declares_reference_abi():
@@ -98,3 +99,37 @@ def test_committed_tuning_table_is_valid():
             li, lj, lk = map(int, k.split(","))
             L.eip_tune_set(li, lj, lk, v)
             L.eip_tune_set_fp32(li, lj, lk, v32)
+
+
+def _noalloc_check(L, li, lj, lk, n_pair, n_aux, spherical=True):
+    f = L.eip_three_center_noalloc_check
+    f.argtypes = [ctypes.c_int] * 5 + [ctypes.c_bool, ctypes.POINTER(ctypes.c_size_t)]
+    f.restype = ctypes.c_int
+    need = ctypes.c_size_t(123)
+    rc = f(li, lj, lk, n_pair, n_aux, spherical, ctypes.byref(need))
+    return rc, need.value
+
+
+def test_noalloc_admission_check_on_host():
+    """The allocation-free entry point's size check runs on the host alone: it
+    accepts what fits its fixed working array and rejects the rest."""
+    if not lib_mod.LIB_PATH.exists():
+        pytest.skip("library not built")
+    L = ctypes.CDLL(str(lib_mod.LIB_PATH))
+    L.eip_noalloc_scratch_bytes.restype = ctypes.c_size_t
+    limit = L.eip_noalloc_scratch_bytes()
+    assert limit == 16 << 20
+    rc, need = _noalloc_check(L, 1, 2, 3, 20, 30)
+    assert rc == 0 and 0 < need <= limit
+    # need grows with the primitive triplets: the class's raw Cartesian plus
+    # spherical block per triplet dominates
+    per = 8 * (3 * 6 * 10 + 3 * 5 * 7)
+    assert need >= 20 * 30 * per
+    rc, need = _noalloc_check(L, 1, 2, 4, 2000, 3000)
+    assert rc == 4 and need > limit
+    rc, need = _noalloc_check(L, 0, 0, 0, 10, 70000)  # small, but beyond the auxiliary-primitive limit
+    assert rc == 4
+    assert _noalloc_check(L, 2, 1, 0, 1, 1)[0] == 1
+    assert _noalloc_check(L, 0, 7, 0, 1, 1)[0] == 1
+    assert _noalloc_check(L, 0, 0, 10, 1, 1)[0] == 1
+    assert _noalloc_check(L, 0, 0, 0, 0, 5) == (0, 0)

@@ -34,6 +34,7 @@ def _bind():
                                                                             ctypes.c_int, ctypes.c_bool,
                                                                             ctypes.c_double, _vp]
     f.restype = ctypes.c_int
+    L.eip_last_error.restype = ctypes.c_char_p
     return L
 
 
@@ -83,6 +84,14 @@ def test_noalloc_rejects_calls_beyond_its_fixed_memory():
     pd = pu.form_pair_data(mol, 1e-14)
     ad = pu.form_auxiliary_pair_data(mol)
     p, a = pd[(1, 2)], ad[4]
+    # the host-side check must already say "too large": only then is the call
+    # made, with an output buffer that a launch would overrun
+    chk = L.eip_three_center_noalloc_check
+    chk.argtypes = [ctypes.c_int] * 5 + [ctypes.c_bool, ctypes.POINTER(ctypes.c_size_t)]
+    chk.restype = ctypes.c_int
+    need = ctypes.c_size_t(0)
+    assert chk(1, 2, 4, p.P_p.shape[0], a.A_a.shape[0], True, ctypes.byref(need)) == 4
     out = torch.zeros(16, dtype=torch.float64, device="cuda")  # never touched on rejection
     assert _noalloc(L, torch, 1, 2, 4, p, a, mol, out) == 4
+    assert b"fixed limit" in L.eip_last_error()
     assert float(out.abs().sum()) == 0.0
