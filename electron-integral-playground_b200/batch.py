@@ -90,6 +90,9 @@ def _bind(L):
     L.eip_batch_stream.restype = _vp
     L.eip_batch_error.argtypes = [_vp]
     L.eip_batch_error.restype = ctypes.c_char_p
+    L.eip_batch_df_plan.argtypes = [_vp, _ipp, _ipp]
+    L.eip_batch_df_gamma.argtypes = [_vp, _vp, _vp]
+    L.eip_batch_df_coulomb.argtypes = [_vp, _vp, _vp]
     L.eip_batch_destroy.argtypes = [_vp]
     L.eip_batch_destroy.restype = None
     L._batch_bound = True
@@ -328,6 +331,25 @@ class ThreeCenterBatch:
                     for t, q0 in enumerate(q_starts):
                         M[p0:p0 + nj, q0:q0 + nk] = buf[s, 0, :, :, t]
         return M
+
+    def df_plan(self):
+        """List the batch's class blocks for the density-fitting contractions
+        (df_gamma / df_coulomb); returns (sum n_ao^2, sum n_aux), the sizes of
+        the concatenated D / J and gamma / c arrays."""
+        n_ao = as_i32([m.n_ao for m in self.molecules])
+        n_aux = as_i32([m.n_aux for m in self.molecules])
+        self._check(self.L.eip_batch_df_plan(self.h, ip(n_ao), ip(n_aux)), "df_plan")
+        return int(np.sum(n_ao.astype(np.int64) ** 2)), int(np.sum(n_aux))
+
+    def df_gamma(self, D_ptr: int, gamma_ptr: int):
+        """gamma_P = sum (mu nu|P) D_{mu nu} of every molecule (device arrays, async)."""
+        self._check(self.L.eip_batch_df_gamma(self.h, ctypes.c_void_p(D_ptr), ctypes.c_void_p(gamma_ptr)),
+                    "df_gamma")
+
+    def df_coulomb(self, c_ptr: int, J_ptr: int):
+        """J_{mu nu} = sum (mu nu|P) c_P of every molecule (device arrays, async)."""
+        self._check(self.L.eip_batch_df_coulomb(self.h, ctypes.c_void_p(c_ptr), ctypes.c_void_p(J_ptr)),
+                    "df_coulomb")
 
     def close(self):
         if self.h:

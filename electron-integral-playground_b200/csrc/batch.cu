@@ -9,8 +9,9 @@
 //   class -> every (l_i, l_j | l_k) class kernel over all molecules at once
 //   (persistent, atomic work list), forked over several streams so classes
 //   overlap.
-// Classes outside the fast kernels' range run as generic raw + transform
-// kernels, one pair per molecule, inside the same graph.
+// Classes outside the fast kernels' range run the general kernel
+// (k_generic.cu) over the same kind of multi-molecule work list, inside the
+// same graph.
 // Point charges (eip_batch_add_charges) form one more ket class, key
 // kPointKet: the nuclear-attraction integrals V[mu nu C] of unit charges, run
 // by the same kernels with a point-charge ket (l_k = 0, one block per charge).
@@ -48,6 +49,7 @@ struct ClassPlan {
     int li, lj, lk;     // lk = kPointKet for point charges
     bool point = false;
     bool fast;
+    int gen_chunks = 1;  // general kernel (not fast): ket-component chunks per block
     int total_items = 0;
     BraTable bra{};
     KetTable ket{};
@@ -112,8 +114,6 @@ struct eip_batch {
     void* d_tables = nullptr;
     size_t table_bytes = 0;
     double* d_etab = nullptr;
-    double* d_scratch = nullptr;
-    size_t scratch_elems = 0;
     double* d_out = nullptr;
     bool own_out = false;
     double* d_checksum = nullptr;
@@ -138,6 +138,10 @@ struct eip_batch {
     bool win_charges = false;
     long long win_elems = 0;
     bool etab_ready = false;
+    // density-fitting plan (eip_batch_df_plan): block list on the device
+    DfBlock* d_df = nullptr;
+    int df_blocks = 0, df_items = 0;
+    long long df_ao2 = 0, df_aux = 0;  // total n_ao^2 and n_aux over the molecules
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     unsigned long long launches_per_run = 0;
@@ -422,6 +426,7 @@ int eip_batch_build(eip_batch* b) {
             pl.point = ac.first == kPointKet;
             const int lk = pl.point ? 0 : pl.lk;
             pl.fast = b->spherical && fast3c_supported(pl.li, pl.lj, lk);
+            if (!pl.fast) pl.gen_chunks = general_chunks(pl.li, pl.lj, lk, pl.point, b->spherical);
             const BraHost& B = bh[pc.first];
             const KetHost& K = kh[ac.first];
             const int ni = b->spherical ? nsph(pl.li) : ncart(pl.li), nj = b->spherical ? nsph(pl.lj) : ncart(pl.lj),
@@ -437,10 +442,7 @@ int eip_batch_build(eip_batch* b) {
                 const long long blk = (long long)nsp * ni * nj * nk * nax;
                 b->out_elems += blk;
                 pl.out_elems += blk;
-                items += (long long)nsp * ((nax + 31) / 32);
-                if (!pl.fast)
-                    b->scratch_elems = std::max(b->scratch_elems, (size_t)nsp * nax * ncart(pl.li) * ncart(pl.lj) *
-                                                                      ncart(lk));
+                items += pl.fast ? (long long)nsp * ((nax + 31) / 32) : (long long)nsp * nax * pl.gen_chunks;
             }
             if (items > 0x7fffffffLL) return fail(b, "too many work items in one class", cudaSuccess);
             pl.total_items = (int)items;
@@ -488,7 +490,9 @@ int eip_batch_build(eip_batch* b) {
         int* spf = &v[5 * (nm + 1)];
         std::vector<int> list64, list32;
         for (int m = 0; m < nm; m++) {
-            const int tiles = (pl.n_auxsh[m] + 31) / 32;
+            // work items per shell pair: tiles of 32 auxiliary shells (fast
+            // kernels) or auxiliary shells x ket chunks (general kernel)
+            const int tiles = pl.fast ? (pl.n_auxsh[m] + 31) / 32 : pl.n_auxsh[m] * pl.gen_chunks;
             int n64 = 0, n32 = 0;
             for (int g = B.sp_begin[m]; g < B.sp_begin[m + 1]; g++) {
                 const bool f32 = mixed && B.bound[g] * K.max_bound[m] * gain < b->fp32_tau;
@@ -533,8 +537,6 @@ int eip_batch_build(eip_batch* b) {
         return fail(b, "E tables", e);
     if ((e = cudaMalloc((void**)&b->d_checksum, sizeof(double) * b->n_mol)) != cudaSuccess)
         return fail(b, "checksums", e);
-    if (b->scratch_elems && (e = cudaMalloc((void**)&b->d_scratch, sizeof(double) * b->scratch_elems)) != cudaSuccess)
-        return fail(b, "generic scratch", e);
     void* h = b->h_tables;
     void* d = b->d_tables;
     for (auto& kv : bh) {
@@ -677,7 +679,7 @@ static int capture(eip_batch* b, bool checksum) {
     int rc = 0;
     cudaMemsetAsync(b->d_checksum, 0, sizeof(double) * b->n_mol, b->stream);
     for (ClassPlan& pl : b->plans)
-        if (pl.fast) cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), b->stream);
+        cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), b->stream);
     for (auto& kv : b->bra_by_class) {
         if (!fast3c_supported(kv.first.first, kv.first.second, 0) || !b->spherical) continue;
         rc |= launch_e_table(kv.first.first, kv.first.second, kv.second, b->d_etab + b->etab_offset[kv.first],
@@ -689,8 +691,7 @@ static int capture(eip_batch* b, bool checksum) {
     int next = 0;
     for (ClassPlan& pl : b->plans) {
         if (pl.total_items == 0 && pl.total_items32 == 0) continue;
-        // generic classes share d_scratch: all of them go to the first side stream
-        cudaStream_t s = pl.fast ? b->side[next++ % n_side] : b->side[0];
+        cudaStream_t s = b->side[next++ % n_side];
         if (pl.fast) {
             if (pl.total_items > 0) {
                 BatchMap map = pl.map;
@@ -709,23 +710,11 @@ static int capture(eip_batch* b, bool checksum) {
                 launches++;
             }
         } else {
-            for (int m = 0; m < b->n_mol; m++) {
-                if (pl.n_sp[m] == 0 || pl.n_auxsh[m] == 0) continue;
-                BraTable bra = pl.bra;
-                bra.n_group = pl.n_sp[m];
-                bra.grp_begin += pl.sp0[m];
-                bra.grp_ao += pl.sp0[m];
-                bra.grp_AB += pl.sp0[m];
-                KetTable ket = pl.ket;
-                ket.n_group = pl.n_auxsh[m];
-                ket.grp_begin += pl.aux0[m];
-                ket.grp_start += pl.aux0[m];
-                const int lk = pl.point ? 0 : pl.lk;
-                rc |= launch_generic_raw(pl.point ? 1 : 0, pl.li, pl.lj, lk, bra, ket, b->omega, 0, b->d_scratch, s);
-                rc |= launch_transform(pl.li, pl.lj, lk, b->spherical, pl.n_sp[m], pl.n_auxsh[m], b->d_scratch,
-                                       b->d_out + pl.out_begin[m], s);
-                launches += 2;
-            }
+            BatchMap map = pl.map;
+            map.checksum = checksum ? b->d_checksum : nullptr;
+            rc |= launch_general(pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, b->spherical, pl.bra, pl.ket, map,
+                                 pl.total_items, b->omega, b->d_out, pl.counter, s);
+            launches++;
         }
     }
     for (int i = 0; i < n_side; i++) {
@@ -757,15 +746,18 @@ int eip_batch_run_class(eip_batch* b, int i_L, int j_L, int k_L) {
     if (!on.ok) return fail(b, "cudaSetDevice (batch device)", cudaErrorInvalidDevice);
     for (ClassPlan& pl : b->plans) {
         if (pl.li != i_L || pl.lj != j_L || pl.lk != k_L) continue;
-        if (!pl.fast || (pl.total_items == 0 && pl.total_items32 == 0)) return 1;
+        if (pl.total_items == 0 && pl.total_items32 == 0) return 1;
         cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), b->stream);
         int rc = 0;
-        if (pl.total_items > 0)
+        if (!pl.fast)
+            rc = launch_general(pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, b->spherical, pl.bra, pl.ket, pl.map,
+                                pl.total_items, b->omega, b->d_out, pl.counter, b->stream);
+        else if (pl.total_items > 0)
             rc |= pl.point ? launch_fast_point(pl.li, pl.lj, pl.bra, pl.ket, pl.map, pl.total_items, b->omega,
                                                b->d_out, pl.counter, b->stream)
                            : launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, pl.map, pl.total_items, b->omega,
                                            b->d_out, pl.counter, b->stream);
-        if (pl.total_items32 > 0)
+        if (pl.fast && pl.total_items32 > 0)
             rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, pl.map32, pl.total_items32, b->omega, b->d_out,
                                 pl.counter32, b->stream, true);
         return rc == 0 ? 0 : fail(b, "class launch", cudaGetLastError());
@@ -818,7 +810,7 @@ long long eip_batch_window_plan(eip_batch* b, const int* fn_lo, const int* fn_hi
                                starts.begin());
                 }
             }
-            const int cnt = s1 - s0, tiles = (cnt + 31) / 32;
+            const int cnt = s1 - s0, tiles = pl.fast ? (cnt + 31) / 32 : cnt * pl.gen_chunks;
             ast[m] = s0;
             acnt[m] = cnt;
             ob[m] = total;
@@ -900,12 +892,12 @@ int eip_batch_run_window(eip_batch* b, double* device_out, int checksum) {
     int next = 0;
     for (ClassPlan& pl : b->plans) {
         if (pl.win_items64 == 0 && pl.win_items32 == 0) continue;
-        cudaStream_t s = pl.fast ? b->side[next++ % n_side] : b->side[0];  // generic: shared scratch
+        cudaStream_t s = b->side[next++ % n_side];
         const int* v = at<int>(dw, pl.win_off);
         const int* ast = v + 2 * (nm + 1);
         const long long* ob = at<long long>(dw, pl.win_off + win_ob_off(nm));
+        cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), s);
         if (pl.fast) {
-            cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), s);
             if (pl.win_items64 > 0) {
                 BatchMap map = pl.map;
                 map.item_begin = v;
@@ -928,23 +920,15 @@ int eip_batch_run_window(eip_batch* b, double* device_out, int checksum) {
                 rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, map, pl.win_items32, b->omega, device_out,
                                     pl.counter32, s, true);
             }
-        } else {
-            const int lk = pl.point ? 0 : pl.lk;
-            for (int m = 0; m < nm; m++) {
-                if (pl.n_sp[m] == 0 || pl.win_count[m] == 0) continue;
-                BraTable bra = pl.bra;
-                bra.n_group = pl.n_sp[m];
-                bra.grp_begin += pl.sp0[m];
-                bra.grp_ao += pl.sp0[m];
-                bra.grp_AB += pl.sp0[m];
-                KetTable ket = pl.ket;
-                ket.n_group = pl.win_count[m];
-                ket.grp_begin += pl.win_start[m];
-                ket.grp_start += pl.win_start[m];
-                rc |= launch_generic_raw(pl.point ? 1 : 0, pl.li, pl.lj, lk, bra, ket, b->omega, 0, b->d_scratch, s);
-                rc |= launch_transform(pl.li, pl.lj, lk, b->spherical, pl.n_sp[m], pl.win_count[m], b->d_scratch,
-                                       device_out + pl.win_out[m], s);
-            }
+        } else if (pl.win_items64 > 0) {
+            BatchMap map = pl.map;
+            map.item_begin = v;
+            map.aux_begin = ast;
+            map.aux_count = ast + nm;
+            map.out_begin = ob;
+            map.checksum = checksum ? b->d_checksum : nullptr;
+            rc |= launch_general(pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, b->spherical, pl.bra, pl.ket, map,
+                                 pl.win_items64, b->omega, device_out, pl.counter, s);
         }
     }
     for (int i = 0; i < n_side; i++) {
@@ -995,7 +979,6 @@ int eip_batch_sync(eip_batch* b) {
 int eip_batch_status(eip_batch* b) {
     if (!b || !b->built) return 2;
     for (const ClassPlan& pl : b->plans) {
-        if (!pl.fast) continue;
         int st[4] = {0, 0, 0, 0};
         cudaError_t e = cudaMemcpyAsync(st, pl.counter, sizeof(st), cudaMemcpyDeviceToHost, b->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
@@ -1009,6 +992,94 @@ int eip_batch_status(eip_batch* b) {
 }
 
 void* eip_batch_stream(eip_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+int eip_batch_df_plan(eip_batch* b, const int* n_ao, const int* n_aux) {
+    if (!b || !b->built || !n_ao || !n_aux) return 2;
+    OnDevice on(b);
+    if (!on.ok) return fail(b, "cudaSetDevice (batch device)", cudaErrorInvalidDevice);
+    const int nm = b->n_mol;
+    std::vector<long long> d_off(nm + 1, 0), g_off(nm + 1, 0);
+    for (int m = 0; m < nm; m++) {
+        if (n_ao[m] < 0 || n_aux[m] < 0) return fail(b, "df_plan: negative size", cudaSuccess);
+        d_off[m + 1] = d_off[m] + (long long)n_ao[m] * n_ao[m];
+        g_off[m + 1] = g_off[m] + n_aux[m];
+        // every function a block touches must lie inside the molecule's n_ao
+        for (auto& kv : b->pairs[m]) {
+            const int ni = b->spherical ? nsph(kv.first.first) : ncart(kv.first.first);
+            const int nj = b->spherical ? nsph(kv.first.second) : ncart(kv.first.second);
+            for (size_t k = 0; k < kv.second.ia.size(); k++)
+                if (kv.second.ia[k] < 0 || kv.second.ja[k] < 0 || kv.second.ia[k] + ni > n_ao[m] ||
+                    kv.second.ja[k] + nj > n_ao[m])
+                    return fail(b, "df_plan: orbital functions beyond n_ao", cudaSuccess);
+        }
+    }
+    std::vector<DfBlock> blocks;
+    long long items = 0;
+    const int rows_per_item = df_rows_per_item();
+    for (const ClassPlan& pl : b->plans) {
+        if (pl.point) continue;
+        const int ni = b->spherical ? nsph(pl.li) : ncart(pl.li), nj = b->spherical ? nsph(pl.lj) : ncart(pl.lj),
+                  nk = b->spherical ? nsph(pl.lk) : ncart(pl.lk);
+        const BraTable& bra = b->bra_by_class[{pl.li, pl.lj}];
+        for (int m = 0; m < nm; m++) {
+            if (pl.n_sp[m] == 0 || pl.n_auxsh[m] == 0) continue;
+            DfBlock bk{};
+            bk.out_off = pl.out_begin[m];
+            bk.d_off = d_off[m];
+            bk.g_off = g_off[m];
+            bk.ao = bra.grp_ao + pl.sp0[m];
+            bk.aux_start = pl.ket.grp_start + pl.aux0[m];
+            bk.nsp = pl.n_sp[m];
+            bk.ni = ni;
+            bk.nj = nj;
+            bk.nk = nk;
+            bk.nax = pl.n_auxsh[m];
+            bk.n_ao = n_ao[m];
+            bk.item0 = (int)items;
+            const std::vector<int>& starts = b->ket_start[pl.lk];
+            if (starts[pl.aux0[m] + pl.n_auxsh[m] - 1] + nk > n_aux[m])
+                return fail(b, "df_plan: auxiliary functions beyond n_aux", cudaSuccess);
+            items += ((long long)bk.nsp * ni * nj + rows_per_item - 1) / rows_per_item;
+            if (items > 0x7fffffffLL) return fail(b, "df_plan: too many work items", cudaSuccess);
+            blocks.push_back(bk);
+        }
+    }
+    cudaError_t e;
+    if (b->d_df) cudaFree(b->d_df);
+    b->d_df = nullptr;
+    if ((e = cudaMalloc((void**)&b->d_df, sizeof(DfBlock) * std::max<size_t>(blocks.size(), 1))) != cudaSuccess)
+        return fail(b, "df_plan: block list", e);
+    if (!blocks.empty() &&
+        (e = cudaMemcpy(b->d_df, blocks.data(), sizeof(DfBlock) * blocks.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(b, "df_plan: block list upload", e);
+    b->df_blocks = (int)blocks.size();
+    b->df_items = (int)items;
+    b->df_ao2 = d_off[nm];
+    b->df_aux = g_off[nm];
+    return 0;
+}
+
+int eip_batch_df_gamma(eip_batch* b, const double* D, double* gamma) {
+    if (!b || !b->built || !b->d_out || !b->d_df || !D || !gamma) return 2;
+    OnDevice on(b);
+    if (!on.ok) return fail(b, "cudaSetDevice (batch device)", cudaErrorInvalidDevice);
+    cudaError_t e = cudaMemsetAsync(gamma, 0, sizeof(double) * b->df_aux, b->stream);
+    if (e != cudaSuccess) return fail(b, "df_gamma: clear", e);
+    if (launch_df_gamma(b->d_df, b->df_blocks, b->df_items, b->d_out, D, gamma, b->stream) != 0)
+        return fail(b, "df_gamma launch", cudaGetLastError());
+    return 0;
+}
+
+int eip_batch_df_coulomb(eip_batch* b, const double* c, double* J) {
+    if (!b || !b->built || !b->d_out || !b->d_df || !c || !J) return 2;
+    OnDevice on(b);
+    if (!on.ok) return fail(b, "cudaSetDevice (batch device)", cudaErrorInvalidDevice);
+    cudaError_t e = cudaMemsetAsync(J, 0, sizeof(double) * b->df_ao2, b->stream);
+    if (e != cudaSuccess) return fail(b, "df_coulomb: clear", e);
+    if (launch_df_coulomb(b->d_df, b->df_blocks, b->df_items, b->d_out, c, J, b->stream) != 0)
+        return fail(b, "df_coulomb launch", cudaGetLastError());
+    return 0;
+}
 
 int eip_batch_copy_output(eip_batch* b, long long offset, long long count, double* host) {
     if (!b || !b->built || !b->d_out || offset < 0 || count < 0 || offset + count > b->out_elems) return 2;
@@ -1029,7 +1100,7 @@ void eip_batch_destroy(eip_batch* b) {
     if (b->h_tables) cudaFreeHost(b->h_tables);
     if (b->d_etab) cudaFree(b->d_etab);
     if (b->d_checksum) cudaFree(b->d_checksum);
-    if (b->d_scratch) cudaFree(b->d_scratch);
+    if (b->d_df) cudaFree(b->d_df);
     if (b->d_win) cudaFree(b->d_win);
     if (b->h_win) cudaFreeHost(b->h_win);
     for (auto ev : b->win_uploaded)

@@ -48,10 +48,32 @@ int launch_fast_point(int li, int lj, const BraTable& bra, const KetTable& ket, 
 int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& ket, const BatchMap& map,
                   int total_items, double omega, double* out, int* counter, cudaStream_t s, bool fp32 = false);
 
-int generic_kc_chunk(int li, int lj, int lk);
-size_t generic_smem_bytes(int li, int lj, int lk, int kc_chunk);
-int launch_generic_raw(int mode, int li, int lj, int lk, const BraTable& bra, const KetTable& ket, double omega,
-                       int skip_lower, double* raw, cudaStream_t s);
+// General kernel (k_generic.cu): any class, run-time angular momenta, over a
+// work list whose items are (shell pair, auxiliary shell or charge, chunk of
+// ket components); molecule m has n_pair * n_aux * general_chunks(...) items
+// numbered from map.item_begin[m], FP64.  point: the ket is unit point charges
+// (lk ignored).  counter[0] must be 0 at launch; counter[1] receives a status.
+// Returns 0, 1 (unsupported class), 2 (CUDA failure) or 3 (too large).
+int general_chunks(int li, int lj, int lk, bool point, bool spherical);
+int launch_general(int li, int lj, int lk, bool point, bool spherical, const BraTable& bra, const KetTable& ket,
+                   const BatchMap& map, int total_items, double omega, double* out, int* counter, cudaStream_t s);
+// One packed class block of one molecule as a density-fitting matrix (df.cu):
+// rows (pair shell, I, J), columns (K, auxiliary shell).
+struct DfBlock {
+    long long out_off;     // first element in the packed buffer
+    long long d_off;       // the molecule's D / J offset (n_ao^2 doubles per molecule)
+    long long g_off;       // the molecule's gamma / c offset (n_aux doubles per molecule)
+    const int2* ao;        // the block's shell pairs: first functions (i0, j0), device
+    const int* aux_start;  // the block's auxiliary shells: first function, device
+    int nsp, ni, nj, nk, nax, n_ao;
+    int item0;             // first work item of the block (df_rows_per_item() rows each)
+};
+int df_rows_per_item();
+// gamma += sum (mu nu|P) D and J += sum (mu nu|P) c over every block (device pointers).
+int launch_df_gamma(const DfBlock* blocks, int n_blocks, int total_items, const double* packed, const double* D,
+                    double* gamma, cudaStream_t s);
+int launch_df_coulomb(const DfBlock* blocks, int n_blocks, int total_items, const double* packed, const double* c,
+                      double* J, cudaStream_t s);
 int launch_overlap_raw(int li, int lj, const BraTable& bra, const double* prim_b, double* raw, cudaStream_t s);
 int launch_transform(int li, int lj, int lk, bool spherical, int n_bra, int n_ket, const double* raw, double* out,
                      cudaStream_t s);

@@ -299,9 +299,14 @@ int stage_inputs(Context& c, const BraInput& bi, const KetInput& ki, Staged& st,
 }
 
 // Computes the compact block of one class into c.d_out and copies it to c.h_out.
-// mode: 0 three-centre, 1 two-centre, 2 nuclear attraction, 3 overlap.
+// mode: 0 three-centre, 1 two-centre (the bra is the one-centre pair class
+// (0, l_P): A = B = P), 2 nuclear attraction (point-charge ket), 3 overlap.
+// Three-centre, two-centre and nuclear attraction run as a batch of one
+// molecule: the fast kernel of the class when there is one (spherical output,
+// pair class l_i <= l_j <= 2 or (0, 3), (0, 4), ket l <= 4), else the general
+// kernel; both write the packed block [pair][I][J][K][ket shell].
 int compute_class(Context& c, int mode, int li, int lj, int lk, bool spherical, double omega, const Staged& st,
-                  size_t n_out, int skip_lower) {
+                  size_t n_out) {
     cudaError_t e = c.d_out.reserve(sizeof(double) * n_out);
     if (e == cudaSuccess) e = c.h_out.reserve(sizeof(double) * n_out);
     if (e != cudaSuccess) {
@@ -312,61 +317,72 @@ int compute_class(Context& c, int mode, int li, int lj, int lk, bool spherical, 
     double* dout = static_cast<double*>(c.d_out.ptr);
     const int n_bra = st.bra.n_group, n_ket = mode == 3 ? 1 : st.ket.n_group;
     cudaEventRecord(c.ev0, c.stream);
-    if (mode == 0 && spherical && fast3c_supported(li, lj, lk)) {
-        // A batch of one molecule: E tables, then the persistent class kernel.
-        const int n_tiles = (n_ket + 31) / 32;
-        const long long items = (long long)n_bra * n_tiles;
-        if (items > 0x7fffffffLL) {
-            set_error("class too large for one call", cudaSuccess);
-            return 2;
-        }
-        const int n_pp = st.n_bra_prims;
-        e = c.d_etab.reserve(sizeof(double) * e_table_doubles(li, lj) * (size_t)n_pp);
-        if (e == cudaSuccess) e = c.d_misc.reserve(256);
-        if (e != cudaSuccess) {
-            set_error("E-table allocation", e);
-            return 2;
-        }
-        BraTable bra = st.bra;
-        bra.prim_E = static_cast<double*>(c.d_etab.ptr);
-        int* misc = static_cast<int*>(c.d_misc.ptr);  // [0] counter, [4..5] item_begin, [8..9] sp, [12..13] aux
-        const int host_misc[16] = {0, 0, 0, 0, 0, (int)items, 0, 0, 0, n_bra, 0, 0, 0, n_ket, 0, 0};
-        cudaMemcpyAsync(misc, host_misc, sizeof(host_misc), cudaMemcpyHostToDevice, c.stream);
-        long long* out_begin = reinterpret_cast<long long*>(misc + 16);
-        cudaMemsetAsync(out_begin, 0, sizeof(long long), c.stream);
-        BatchMap map{1, misc + 4, misc + 8, misc + 12, out_begin, nullptr, nullptr, nullptr};
-        rc = launch_e_table(li, lj, bra, static_cast<double*>(c.d_etab.ptr), c.stream);
-        if (rc == 0) rc = launch_fast3c(li, lj, lk, bra, st.ket, map, (int)items, omega, dout, misc, c.stream);
-        c.launches += 2;
-        int status[2] = {0, 0};
-        if (rc == 0) e = cudaMemcpyAsync(status, misc, sizeof(status), cudaMemcpyDeviceToHost, c.stream);
-        if (rc == 0 && e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
-        if (rc == 0 && (e != cudaSuccess || status[1] != 0)) {
-            snprintf(g_last_error, sizeof g_last_error, "fast (mu nu|P) kernel self-check %d (cuda: %s)", status[1],
-                     cudaGetErrorString(e));
-            fprintf(stderr, "[eip] %s\n", g_last_error);
-            return 2;
-        }
-    } else {
-        const size_t n_raw = (size_t)n_bra * n_ket * ncart(li) * ncart(lj) * ncart(lk);
+    if (mode == 3) {
+        const size_t n_raw = (size_t)n_bra * ncart(li) * ncart(lj);
         e = c.d_raw.reserve(sizeof(double) * n_raw);
         if (e != cudaSuccess) {
             set_error("scratch allocation", e);
             return 2;
         }
         double* raw = static_cast<double*>(c.d_raw.ptr);
-        if (mode == 3) {
-            rc = launch_overlap_raw(li, lj, st.bra, st.prim_b, raw, c.stream);
-        } else {
-            if (skip_lower) cudaMemsetAsync(raw, 0, sizeof(double) * n_raw, c.stream);
-            rc = launch_generic_raw(mode == 2 ? 1 : 0, li, lj, lk, st.bra, st.ket, omega, skip_lower, raw, c.stream);
-        }
-        if (rc == 0) rc = launch_transform(li, lj, lk, spherical, n_bra, n_ket, raw, dout, c.stream);
+        rc = launch_overlap_raw(li, lj, st.bra, st.prim_b, raw, c.stream);
+        if (rc == 0) rc = launch_transform(li, lj, 0, spherical, n_bra, 1, raw, dout, c.stream);
         c.launches += 2;
-    }
-    if (rc != 0) {
-        set_error("kernel launch", cudaGetLastError());
-        return 2;
+        if (rc != 0) {
+            set_error("kernel launch", cudaGetLastError());
+            return 2;
+        }
+    } else {
+        const bool point = mode == 2;
+        const bool fast = spherical && fast3c_supported(li, lj, point ? 0 : lk);
+        const long long items = fast ? (long long)n_bra * ((n_ket + 31) / 32)
+                                     : (long long)n_bra * n_ket * general_chunks(li, lj, lk, point, spherical);
+        if (items > 0x7fffffffLL) {
+            set_error("class too large for one call", cudaSuccess);
+            return 2;
+        }
+        e = c.d_misc.reserve(256);
+        if (e == cudaSuccess && fast)
+            e = c.d_etab.reserve(sizeof(double) * e_table_doubles(li, lj) * (size_t)st.n_bra_prims);
+        if (e != cudaSuccess) {
+            set_error("work-list allocation", e);
+            return 2;
+        }
+        // one-molecule work map: [0..1] counter/status, [4..5] item_begin,
+        // [8..9] pair begin, [12..13] ket begin, then out_begin (= 0)
+        int* misc = static_cast<int*>(c.d_misc.ptr);
+        const int host_misc[16] = {0, 0, 0, 0, 0, (int)items, 0, 0, 0, n_bra, 0, 0, 0, n_ket, 0, 0};
+        cudaMemcpyAsync(misc, host_misc, sizeof(host_misc), cudaMemcpyHostToDevice, c.stream);
+        long long* out_begin = reinterpret_cast<long long*>(misc + 16);
+        cudaMemsetAsync(out_begin, 0, sizeof(long long), c.stream);
+        BatchMap map{1, misc + 4, misc + 8, misc + 12, out_begin, nullptr, nullptr, nullptr};
+        if (fast) {
+            BraTable bra = st.bra;
+            bra.prim_E = static_cast<double*>(c.d_etab.ptr);
+            rc = launch_e_table(li, lj, bra, static_cast<double*>(c.d_etab.ptr), c.stream);
+            if (rc == 0)
+                rc = point ? launch_fast_point(li, lj, bra, st.ket, map, (int)items, omega, dout, misc, c.stream)
+                           : launch_fast3c(li, lj, lk, bra, st.ket, map, (int)items, omega, dout, misc, c.stream);
+            c.launches += 2;
+        } else {
+            rc = launch_general(li, lj, lk, point, spherical, st.bra, st.ket, map, (int)items, omega, dout, misc,
+                                c.stream);
+            c.launches += 1;
+        }
+        if (rc != 0) {
+            set_error(rc == 3 ? "class needs more shared memory than a CTA has" : "kernel launch",
+                      cudaGetLastError());
+            return 2;
+        }
+        int status[2] = {0, 0};
+        e = cudaMemcpyAsync(status, misc, sizeof(status), cudaMemcpyDeviceToHost, c.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+        if (e != cudaSuccess || status[1] != 0) {
+            snprintf(g_last_error, sizeof g_last_error, "integral kernel self-check %d (cuda: %s)", status[1],
+                     cudaGetErrorString(e));
+            fprintf(stderr, "[eip] %s\n", g_last_error);
+            return 2;
+        }
     }
     cudaEventRecord(c.ev1, c.stream);
     e = cudaMemcpyAsync(c.h_out.ptr, dout, sizeof(double) * n_out, cudaMemcpyDeviceToHost, c.stream);
@@ -472,7 +488,7 @@ int three_center(const int i_L, const int j_L, const int k_L, const double* pair
               nk = spherical ? nsph(k_L) : ncart(k_L);
     const int nb = st.bra.n_group, nkt = st.ket.n_group;
     const size_t n_out = (size_t)nb * ni * nj * nk * nkt;
-    if (int rc = compute_class(c, 0, i_L, j_L, k_L, spherical, omega, st, n_out, 0)) return rc;
+    if (int rc = compute_class(c, 0, i_L, j_L, k_L, spherical, omega, st, n_out)) return rc;
     const double* h = static_cast<const double*>(c.h_out.ptr);
     const size_t nao = (size_t)n_ao, nao2 = nao * nao;
 #pragma omp parallel for schedule(dynamic, 16)
@@ -511,9 +527,10 @@ int two_center(const int i_L, const int j_L, const double* aux_A_a, const double
     const int ni = spherical ? nsph(i_L) : ncart(i_L), nk = spherical ? nsph(j_L) : ncart(j_L);
     const int nb = st.bra.n_group, nkt = st.ket.n_group;
     const size_t n_out = (size_t)nb * ni * nk * nkt;
-    // reference skip: same class and i_aux_start > j_aux_start (MI/two_center.cpp:136-138)
+    // reference skip: same class and i_aux_start > j_aux_start (MI/two_center.cpp:136-138);
+    // every block is computed, the skipped ones are not scattered
     const int skip = i_L == j_L ? 1 : 0;
-    if (int rc = compute_class(c, 1, i_L, 0, j_L, spherical, omega, st, n_out, skip)) return rc;
+    if (int rc = compute_class(c, 1, 0, i_L, j_L, spherical, omega, st, n_out)) return rc;
     const double* h = static_cast<const double*>(c.h_out.ptr);
     const size_t na = (size_t)n_aux;
 #pragma omp parallel for schedule(dynamic, 8)
@@ -552,7 +569,7 @@ int nuclear_attraction(const int i_L, const int j_L, const double* pair_P_p, con
     const int ni = spherical ? nsph(i_L) : ncart(i_L), nj = spherical ? nsph(j_L) : ncart(j_L);
     const int nb = st.bra.n_group, nc = n_charge;
     const size_t n_out = (size_t)nb * ni * nj * nc;
-    if (int rc = compute_class(c, 2, i_L, j_L, 0, spherical, omega, st, n_out, 0)) return rc;
+    if (int rc = compute_class(c, 2, i_L, j_L, 0, spherical, omega, st, n_out)) return rc;
     const double* h = static_cast<const double*>(c.h_out.ptr);
     const size_t nao = (size_t)n_ao;
 #pragma omp parallel for schedule(dynamic, 16)
@@ -598,7 +615,7 @@ int overlap(const int i_L, const int j_L, const double* pair_A_a, const double* 
     const int ni = spherical ? nsph(i_L) : ncart(i_L), nj = spherical ? nsph(j_L) : ncart(j_L);
     const int nb = st.bra.n_group;
     const size_t n_out = (size_t)nb * ni * nj;
-    if (int rc = compute_class(c, 3, i_L, j_L, 0, spherical, 0.0, st, n_out, 0)) return rc;
+    if (int rc = compute_class(c, 3, i_L, j_L, 0, spherical, 0.0, st, n_out)) return rc;
     const double* h = static_cast<const double*>(c.h_out.ptr);
     const size_t nao = (size_t)n_ao;
     for (int b = 0; b < nb; b++) {

@@ -18,9 +18,25 @@
 //     coefficients come from a per-l_k constant-memory table (KetCoefTable),
 //     so all warps run the same ket/bra code (instruction-cache friendly);
 //     zero coefficients are skipped by a warp-uniform branch;
-//   * E^{ij}_t tables of each primitive pair are precomputed once into the
+//   * E tables of each primitive pair are precomputed once into the
 //     device-resident pair table (e_table_kernel) and staged per pair into
 //     shared memory;
+//   * FP64 kernels of pair classes with l_i > 0 accumulate the (0, b)
+//     functions of the pair (l_j <= |b| <= l_i + l_j, Hermite coefficients
+//     E^{0 b}_t around P of a Gaussian on centre B) and move l_i onto centre A
+//     once per contracted block, in the epilogue, by the transfer
+//     (a+1_d, b) = (a, b+1_d) - AB_d (a, b); AB is the same for every
+//     primitive pair of a shell pair, so the transfer commutes with the
+//     contraction over primitives and the per-unit bra work drops (p-d: 77
+//     instead of 108 E-term products per ket component, d-d: 203 instead of
+//     276).  The FP32 kernels of the mixed-precision path keep the E^{ij}_t
+//     tables (transferred per primitive pair in FP64), so that no FP32
+//     cancellation in the transfer enters their error budget;
+//   * spherical kets read only the top Hermite level |s| = l_k of the
+//     tetrahedron: a real solid harmonic is a harmonic polynomial, so the
+//     Hermite expansion of its Gaussian has no lower terms (checked at compile
+//     time on the coefficient tables), and tetrahedron entries of order < l_k
+//     are neither computed nor stored;
 //   * one-warp CTAs (most low-l classes) keep the unit's Boys values in
 //     registers and load the next unit's data while evaluating the current one;
 //   * primitive pairs are reduced in registers: each contracted block is
@@ -43,20 +59,40 @@ constexpr int kVariants = 6;
 __host__ __device__ constexpr int variant_acc(int v) { return v == 2 || v == 4 ? 24 : (v == 3 ? 96 : 48); }
 __host__ __device__ constexpr int variant_warps(int v) { return v == 1 || v == 3 ? 8 : (v >= 4 ? 24 : 16); }
 
-template <int LI, int LJ, int LK, int V = 0>
+// E table record of one primitive pair (e_table_kernel): for l_i > 0 first
+// E^{0 b}_t, b <= l_i + l_j, for x, y, z (the transfer-after-contraction
+// kernels), then E^{i j}_t for x, y, z (the direct kernels).
+template <int LI, int LJ>
+__host__ __device__ constexpr int e_hrr_size() { return LI > 0 ? (LI + LJ + 1) * (LI + LJ + 2) / 2 : 0; }
+template <int LI, int LJ>
+__host__ __device__ constexpr int e_record() { return 3 * (e_hrr_size<LI, LJ>() + e_size<LI, LJ>()); }
+
+// FP64 kernels of pair classes with l_i > 0 transfer after the contraction.
+template <int LI, typename T>
+constexpr bool use_hrr() { return LI > 0 && std::is_same<T, double>::value; }
+
+template <int LI, int LJ, int LK, int V = 0, bool HRR = false>
 struct Fast3c {
     static constexpr int L = LI + LJ + LK;
     static constexpr int LIJ = LI + LJ;
     static constexpr int NI = ncart(LI), NJ = ncart(LJ), NIJ = NI * NJ;
     static constexpr int NIJS = nsph(LI) * nsph(LJ);
     static constexpr int NKO = nsph(LK);
-    static constexpr int KPW_MAX = (variant_acc(V) / NIJ) < 1 ? 1 : (variant_acc(V) / NIJ);
+    // bra functions accumulated per ket component: (0, b) functions with
+    // l_j <= |b| <= l_i + l_j (transfer after contraction) or the (i, j) pairs
+    static constexpr int NB = HRR ? nherm(LIJ) - nherm(LJ - 1) : NIJ;
+    static constexpr int KPW_MAX = (variant_acc(V) / NB) < 1 ? 1 : (variant_acc(V) / NB);
     static constexpr int KS = (NKO + KPW_MAX - 1) / KPW_MAX;  // warps per CTA
     static constexpr int KPW = (NKO + KS - 1) / KS;           // ket components per warp
     static constexpr int NR = nherm(L);
-    static constexpr int RPW = (NR + KS - 1) / KS;            // R entries per warp
+    static constexpr int R0 = nherm(LK - 1);                  // first tetrahedron entry read by the ket
+    static constexpr int NRN = NR - R0;                       // entries computed and stored
+    static constexpr int RPW = (NRN + KS - 1) / KS;           // R entries per warp
     static constexpr int NHB = nherm(LIJ);
-    static constexpr int NE = e_size<LI, LJ>();
+    // E entries per axis read per unit: E^{0 b}_t (transfer) or E^{i j}_t
+    static constexpr int NE = HRR ? e_hrr_size<LI, LJ>() : e_size<LI, LJ>();
+    // offset of those entries in a primitive pair's E record
+    static constexpr int E_OFF = HRR ? 0 : 3 * e_hrr_size<LI, LJ>();
     static constexpr int THREADS = 32 * KS;
     // resident CTAs per SM asked of the register allocator
     static constexpr int MIN_CTAS = (variant_warps(V) / KS) < 1 ? 1 : (variant_warps(V) / KS);
@@ -65,7 +101,7 @@ struct Fast3c {
     static constexpr int NU = L + 6;
     template <typename T>
     static constexpr size_t smem_bytes() {
-        return (KS == 1 ? 0 : sizeof(double) * UB * NU * 32) + sizeof(T) * (NR * 32 + UB * 3 * NE);
+        return (KS == 1 ? 0 : sizeof(double) * UB * NU * 32) + sizeof(T) * (NRN * 32 + UB * 3 * NE);
     }
 };
 
@@ -99,6 +135,18 @@ constexpr KetCoefTable<LK> make_ket_table() {
 }
 template <int LK>
 __constant__ KetCoefTable<LK> c_ket_coef = make_ket_table<LK>();
+
+// True when every coefficient of the ket levels below |s| = l_k is exactly
+// zero in the tables (spherical kets, l_k <= 4); the kernels then read only the
+// top level.
+template <int LK>
+constexpr bool ket_top_level_only() {
+    const KetCoefTable<LK> t = make_ket_table<LK>();
+    for (int ko = 0; ko < nsph(LK); ko++)
+        for (int i = ncart(LK); i < ket_n_s(LK); i++)
+            if (t.v[ko][i] != 0.0) return false;
+    return true;
+}
 
 // Two-centre E^{i,j}_t along one axis for i <= LI, j <= LJ:
 // vertical recursion E^{i+1,0}_t = E^{i,0}_{t-1}/(2p) + PA E^{i,0}_t + (t+1) E^{i,0}_{t+1},
@@ -138,20 +186,80 @@ __device__ __forceinline__ void bra_e_table(double PA, double AB, double inv2p, 
             for (int t = 0; t <= i + j; t++) out[e_offset<LJ>(i, j) + t] = W[i][j][t];
 }
 
-// Fill bra.prim_E: one thread per shell pair, looping over its primitive pairs.
+// E^{0,b}_t along one axis for b <= N, a Gaussian on centre B expanded about
+// P: E^{0,b+1}_t = E^{0,b}_{t-1}/(2p) + PB E^{0,b}_t + (t+1) E^{0,b}_{t+1},
+// out[b (b+1)/2 + t].
+template <int N>
+__device__ __forceinline__ void bra_e0b_table(double PB, double inv2p, double* out) {
+    double W[N + 1][N + 1];
+#pragma unroll
+    for (int b = 0; b <= N; b++)
+#pragma unroll
+        for (int t = 0; t <= N; t++) W[b][t] = 0.0;
+    W[0][0] = 1.0;
+#pragma unroll
+    for (int b = 0; b < N; b++)
+#pragma unroll
+        for (int t = 0; t <= b + 1; t++) {
+            double v = 0.0;
+            if (t >= 1) v = inv2p * W[b][t - 1];
+            if (t <= b) v = fma(PB, W[b][t], v);
+            if (t + 1 <= b) v = fma((double)(t + 1), W[b][t + 1], v);
+            W[b + 1][t] = v;
+        }
+#pragma unroll
+    for (int b = 0; b <= N; b++)
+#pragma unroll
+        for (int t = 0; t <= b; t++) out[b * (b + 1) / 2 + t] = W[b][t];
+}
+
+// Fill bra.prim_E (records of e_record<LI, LJ>() doubles per primitive pair):
+// one thread per shell pair, looping over its primitive pairs.
 template <int LI, int LJ>
 __global__ void e_table_kernel(BraTable bra, double* __restrict__ prim_E) {
     constexpr int NE = e_size<LI, LJ>();
+    constexpr int NH = e_hrr_size<LI, LJ>();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= bra.n_group) return;
     const double4 AB = bra.grp_AB[g];
     for (int pp = bra.grp_begin[g]; pp < bra.grp_begin[g + 1]; pp++) {
         const double4 PA = bra.prim_PA[pp];
         const double inv2p = 0.5 / bra.prim_P[pp].w;
-        double* out = prim_E + (size_t)pp * 3 * NE;
+        double* out = prim_E + (size_t)pp * e_record<LI, LJ>();
+        if constexpr (NH > 0) {
+            bra_e0b_table<LI + LJ>(PA.x + AB.x, inv2p, out);
+            bra_e0b_table<LI + LJ>(PA.y + AB.y, inv2p, out + NH);
+            bra_e0b_table<LI + LJ>(PA.z + AB.z, inv2p, out + 2 * NH);
+            out += 3 * NH;
+        }
         bra_e_table<LI, LJ>(PA.x, AB.x, inv2p, out);
         bra_e_table<LI, LJ>(PA.y, AB.y, inv2p, out + NE);
         bra_e_table<LI, LJ>(PA.z, AB.z, inv2p, out + 2 * NE);
+    }
+}
+
+// Index of the (0, b) function b = (bx, by, bz) among those with
+// LJ <= |b| (order-major, x-major descending within an order).
+template <int LJ>
+__host__ __device__ constexpr int base_index(int bx, int by, int bz) {
+    return herm_index(bx, by, bz) - nherm(LJ - 1);
+}
+
+// Cartesian (a, b) block entry, |a| = AX+AY+AZ, from the accumulated (0, b)
+// functions by the transfer (a+1_d, b) = (a, b+1_d) - AB_d (a, b).
+template <int LJ, int AX, int AY, int AZ, int BX, int BY, int BZ, typename T, typename Acc>
+__device__ __forceinline__ T hrr_value(const Acc& acc, int c, T abx, T aby, T abz) {
+    if constexpr (AX + AY + AZ == 0) {
+        return acc[base_index<LJ>(BX, BY, BZ)][c];
+    } else if constexpr (AX > 0) {
+        return hrr_value<LJ, AX - 1, AY, AZ, BX + 1, BY, BZ, T>(acc, c, abx, aby, abz) -
+               abx * hrr_value<LJ, AX - 1, AY, AZ, BX, BY, BZ, T>(acc, c, abx, aby, abz);
+    } else if constexpr (AY > 0) {
+        return hrr_value<LJ, AX, AY - 1, AZ, BX, BY + 1, BZ, T>(acc, c, abx, aby, abz) -
+               aby * hrr_value<LJ, AX, AY - 1, AZ, BX, BY, BZ, T>(acc, c, abx, aby, abz);
+    } else {
+        return hrr_value<LJ, AX, AY, AZ - 1, BX, BY, BZ + 1, T>(acc, c, abx, aby, abz) -
+               abz * hrr_value<LJ, AX, AY, AZ - 1, BX, BY, BZ, T>(acc, c, abx, aby, abz);
     }
 }
 
@@ -192,10 +300,13 @@ __device__ __forceinline__ void unit_prefactor(double p, double q, double c, dou
 // zeta = p (omega > 0: p w^2 / (p + w^2)), prefactor c_ab 2 pi / p
 // (omega > 0: c_ab 2 pi w / (p sqrt(p + w^2))), l_k = 0.
 template <int LI, int LJ, int LK, int V, typename T, bool POINT = false>
-__global__ void __launch_bounds__(Fast3c<LI, LJ, LK, V>::THREADS, Fast3c<LI, LJ, LK, V>::MIN_CTAS)
+__global__ void __launch_bounds__(Fast3c<LI, LJ, LK, V, use_hrr<LI, T>()>::THREADS,
+                                  Fast3c<LI, LJ, LK, V, use_hrr<LI, T>()>::MIN_CTAS)
 k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, BatchMap map, double omega,
          double* __restrict__ out, int* __restrict__ work_counter, int total_items) {
-    using C = Fast3c<LI, LJ, LK, V>;
+    constexpr bool HRR = use_hrr<LI, T>();
+    using C = Fast3c<LI, LJ, LK, V, HRR>;
+    static_assert(POINT || ket_top_level_only<LK>(), "spherical ket with lower Hermite levels");
     constexpr int L = C::L;
     constexpr int UB = C::UB;
     constexpr int NU = C::NU;
@@ -205,7 +316,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
     // unit, then the units' E tables
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sU = reinterpret_cast<double*>(smem_raw);                   // [UB][NU][32], KS > 1
-    T* sR = reinterpret_cast<T*>(sU + (C::KS == 1 ? 0 : UB * NU * 32));  // [NR][32]
+    T* sR = reinterpret_cast<T*>(sU + (C::KS == 1 ? 0 : UB * NU * 32));  // [NRN][32], entries R0..NR-1
     T* sE = sR + C::NR * 32;                            // [UB][3 NE]
     __shared__ int s_item;
 
@@ -266,9 +377,9 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
             continue;
         }
 
-        T acc[C::NIJ][C::KPW];
+        T acc[C::NB][C::KPW];
 #pragma unroll
-        for (int i = 0; i < C::NIJ; i++)
+        for (int i = 0; i < C::NB; i++)
 #pragma unroll
             for (int c = 0; c < C::KPW; c++) acc[i][c] = T(0);
 
@@ -283,6 +394,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
         // evaluated, so a unit's global loads are off its dependency chain;
         // warp barriers replace block barriers.
         constexpr int NE3 = 3 * C::NE;
+        constexpr int ERS = e_record<LI, LJ>();
         constexpr bool ONE = C::KS == 1;
         constexpr int EPL = ONE ? (NE3 + 31) / 32 : 1;  // E values per lane
         double4 nP, nC;
@@ -299,7 +411,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
 #pragma unroll
             for (int r = 0; r < EPL; r++) {
                 const int e = lane + 32 * r;
-                nE[r] = e < NE3 ? __ldg(bra.prim_E + (size_t)fpp * NE3 + e) : 0.0;
+                nE[r] = e < NE3 ? __ldg(bra.prim_E + (size_t)fpp * ERS + C::E_OFF + e) : 0.0;
             }
             if (++fkk == nk_max) {
                 fkk = 0;
@@ -344,7 +456,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 for (int e = threadIdx.x; e < nb * NE3; e += C::THREADS) {
                     const int ub = e / NE3, r = e - ub * NE3;
                     const int pp = pb + (nk_max == 1 ? u0 + ub : (u0 + ub) / nk_max);
-                    sE[e] = (T)__ldg(bra.prim_E + (size_t)pp * NE3 + r);
+                    sE[e] = (T)__ldg(bra.prim_E + (size_t)pp * ERS + C::E_OFF + r);
                 }
                 for (int ub = warp; ub < nb; ub += C::KS) {
                     const int u = u0 + ub;
@@ -400,8 +512,8 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 }
                 static_for<0, C::KS>([&](auto g) {
                     constexpr int G = decltype(g)::value;
-                    constexpr int lo_e = G * C::RPW;
-                    constexpr int hi_e = (G + 1) * C::RPW < C::NR ? (G + 1) * C::RPW : C::NR;
+                    constexpr int lo_e = C::R0 + G * C::RPW;
+                    constexpr int hi_e = C::R0 + ((G + 1) * C::RPW < C::NRN ? (G + 1) * C::RPW : C::NRN);
                     if (warp == G) {
                         static_for<lo_e, hi_e>([&](auto e) {
                             constexpr int idx = decltype(e)::value;
@@ -424,7 +536,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                                 constexpr T h = (T)hermite_r_coef(t, mx);
                                 r = fma(h * px[2 * mx - t], ry, r);
                             });
-                            sR[idx * 32 + lane] = r;
+                            sR[(idx - C::R0) * 32 + lane] = r;
                         });
                     }
                 });
@@ -450,6 +562,44 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 // bra: acc[ij][c0 + c] += pref * sum_t Ex sum_u Ey sum_v Ez X[c][tuv], c < NC
                 auto bra_acc = [&](const auto& X, auto c0_, auto nc_) {
                     constexpr int c0 = decltype(c0_)::value, NC = decltype(nc_)::value;
+                    if constexpr (HRR) {
+                        // (0, b) functions: acc[b][c0 + c] += pref sum_t E^{0bx}_t sum_u E^{0by}_u
+                        // sum_v E^{0bz}_v X[c][tuv], E^{0b}_t at b (b+1)/2 + t per axis
+                        static_for<0, C::NB>([&](auto b_) {
+                            constexpr int bi = decltype(b_)::value;
+                            constexpr int bx = herm_t(nherm(LJ - 1) + bi), by = herm_u(nherm(LJ - 1) + bi),
+                                          bz = herm_v(nherm(LJ - 1) + bi);
+                            T sxv[NC];
+#pragma unroll
+                            for (int c = 0; c < NC; c++) sxv[c] = T(0);
+                            static_for<0, bx + 1>([&](auto t_) {
+                                constexpr int t = decltype(t_)::value;
+                                T su[NC];
+#pragma unroll
+                                for (int c = 0; c < NC; c++) su[c] = T(0);
+                                static_for<0, by + 1>([&](auto u_) {
+                                    constexpr int u = decltype(u_)::value;
+                                    T sv[NC];
+#pragma unroll
+                                    for (int c = 0; c < NC; c++) sv[c] = T(0);
+                                    static_for<0, bz + 1>([&](auto v_) {
+                                        constexpr int v = decltype(v_)::value;
+                                        const T ez = sEu[2 * C::NE + bz * (bz + 1) / 2 + v];
+#pragma unroll
+                                        for (int c = 0; c < NC; c++) sv[c] = fma(ez, X[c][herm_index(t, u, v)], sv[c]);
+                                    });
+                                    const T ey = sEu[C::NE + by * (by + 1) / 2 + u];
+#pragma unroll
+                                    for (int c = 0; c < NC; c++) su[c] = fma(ey, sv[c], su[c]);
+                                });
+                                const T ex = sEu[bx * (bx + 1) / 2 + t];
+#pragma unroll
+                                for (int c = 0; c < NC; c++) sxv[c] = fma(ex, su[c], sxv[c]);
+                            });
+#pragma unroll
+                            for (int c = 0; c < NC; c++) acc[bi][c0 + c] = fma(pref, sxv[c], acc[bi][c0 + c]);
+                        });
+                    } else
                     static_for<0, C::NI>([&](auto ci_) {
                         constexpr int ci = decltype(ci_)::value;
                         constexpr int ix = cart_x(LI, ci), iy = cart_y(LI, ci), iz = cart_z(LI, ci);
@@ -511,7 +661,8 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                         static_for<0, C::NHB>([&](auto h_) {
                             constexpr int h = decltype(h_)::value;
                             constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
-                            static_for<0, LK / 2 + 1>([&](auto j_) {
+                            // top Hermite level |s| = LK only (ket_top_level_only)
+                            static_for<0, 1>([&](auto j_) {
                                 constexpr int j = decltype(j_)::value;
                                 constexpr int S = LK - 2 * j;
                                 T part[NC];
@@ -526,7 +677,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                                         return false;
                                     }();
                                     if constexpr (any) {
-                                        const T r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
+                                        const T r = sR[(herm_index(t + sx, u + sy, v + sz) - C::R0) * 32 + lane];
                                         static_for<0, NC>([&](auto c_) {
                                             constexpr int c = decltype(c_)::value;
                                             constexpr double kc = ket_sph_coef(LK, c0 + c, sx, sy, sz);
@@ -549,7 +700,8 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
 #pragma unroll
                         for (int h = 0; h < C::NHB; h++) Xh[c][h] = T(0);
                     int sidx = 0;
-                    static_for<0, LK / 2 + 1>([&](auto j_) {
+                    // top Hermite level |s| = LK only (ket_top_level_only)
+                    static_for<0, 1>([&](auto j_) {
                         constexpr int j = decltype(j_)::value;
                         constexpr int S = LK - 2 * j;
                         static_for<0, ncart(S)>([&](auto sc_) {
@@ -568,7 +720,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                                 static_for<0, C::NHB>([&](auto h_) {
                                     constexpr int h = decltype(h_)::value;
                                     constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
-                                    const T r = sR[herm_index(t + sx, u + sy, v + sz) * 32 + lane];
+                                    const T r = sR[(herm_index(t + sx, u + sy, v + sz) - C::R0) * 32 + lane];
 #pragma unroll
                                     for (int c = 0; c < C::KPW; c++) Xh[c][h] = fma(ce[c], r, Xh[c][h]);
                                 });
@@ -583,13 +735,30 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
             }
         }
 
-        // Epilogue: bra Cartesian -> spherical, coalesced packed stores.
+        // Epilogue: (transfer l_i onto A,) bra Cartesian -> spherical, coalesced
+        // packed stores.
         const size_t obase = (size_t)__ldg(map.out_begin + m);
         double wsum = 0.0;
+        T abx = T(0), aby = T(0), abz = T(0);
+        if constexpr (HRR) {
+            const double4 AB = bra.grp_AB[sp];
+            abx = (T)AB.x;
+            aby = (T)AB.y;
+            abz = (T)AB.z;
+        }
         static_for<0, C::KPW>([&](auto c_) {
             constexpr int c = decltype(c_)::value;
             const int ko = warp * C::KPW + c;
             if (ko < C::NKO) {
+                // Cartesian (i, j) entry of ket component c
+                auto cart_ij = [&](auto ci_, auto cj_) -> T {
+                    constexpr int ci = decltype(ci_)::value, cj = decltype(cj_)::value;
+                    if constexpr (HRR)
+                        return hrr_value<LJ, cart_x(LI, ci), cart_y(LI, ci), cart_z(LI, ci), cart_x(LJ, cj),
+                                         cart_y(LJ, cj), cart_z(LJ, cj), T>(acc, c, abx, aby, abz);
+                    else
+                        return acc[ci * C::NJ + cj][c];
+                };
                 static_for<0, nsph(LI)>([&](auto I_) {
                     constexpr int I = decltype(I_)::value;
                     static_for<0, nsph(LJ)>([&](auto J_) {
@@ -603,7 +772,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                                 static_for<0, C::NJ>([&](auto cj_) {
                                     constexpr int cj = decltype(cj_)::value;
                                     constexpr double wj = sph_coef(LJ, J, cj);
-                                    if constexpr (wj != 0.0) vj = fma((T)wj, acc[ci * C::NJ + cj][c], vj);
+                                    if constexpr (wj != 0.0) vj = fma((T)wj, cart_ij(ci_, cj_), vj);
                                 });
                                 v = fma((T)wi, vj, v);
                             }
@@ -630,7 +799,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
 template <int LI, int LJ, int LK, int V, typename T, bool POINT = false>
 static int launch_one(const double* boys_table, const BraTable& bra, const KetTable& ket, const BatchMap& map,
                       int total_items, double omega, double* out, int* counter, cudaStream_t s) {
-    using C = Fast3c<LI, LJ, LK, V>;
+    using C = Fast3c<LI, LJ, LK, V, use_hrr<LI, T>()>;
     if (total_items <= 0) return 0;
     constexpr size_t smem = C::template smem_bytes<T>();
     static std::atomic<int> max_blocks[kMaxDevices];

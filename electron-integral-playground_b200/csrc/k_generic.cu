@@ -1,25 +1,48 @@
-// Generic kernels: any supported angular class with run-time angular momenta.
+// General kernels: every angular class the C ABI accepts, with run-time
+// angular momenta (orbital l <= 6, auxiliary l <= 9; reference
+// c_library/angular.h:3-4), over the same multi-molecule work list as the fast
+// kernels.  They carry what the fast templated kernels do not: Cartesian
+// output, (mu nu|P) classes beyond d-d|g, the high-l metric and
+// nuclear-attraction classes.
 //
-// They cover what the fast templated kernels do not (Cartesian output,
-// (mu nu|P) classes beyond d-d|g, every (P|Q) and nuclear-attraction class) and
-// are the correctness fallback for the whole C ABI range (orbital l <= 6,
-// auxiliary l <= 9; reference c_library/angular.h:3-4).
+// general_kernel: persistent CTAs of kGenThreads threads; one work item is
+// one contracted block (shell pair, auxiliary shell or point charge, chunk of
+// ket components), computed as
+//   (mu nu|P) = sum_{prim pairs} sum_{aux prims} pref
+//               sum_{tuv} E^{0 b}_{tuv} sum_s (-1)^{|s|} E^{k}_s R_{t+s_x,u+s_y,v+s_z}
+// for the (0, b) functions of the pair (all b with l_j <= |b| <= l_i + l_j, a
+// Gaussian on centre B of exponent p = a + b), followed once per block by the
+// horizontal transfer (a+1_d, b) = (a, b+1_d) - AB_d (a, b) that moves l_i
+// onto centre A.  AB is the same for every primitive pair of a shell pair, so
+// the transfer commutes with the contraction over primitives (this library's
+// arrangement; the reference transfers E coefficients per primitive pair,
+// c_library/mcmurchie_davidson_E_term.hpp:166-199).  Per block of kGenUB
+// units (primitive pair x auxiliary primitive) the CTA first evaluates, one
+// thread per unit, the prefactor, Boys function, scaled R^{(m)}_000 and
+// coordinate powers, and per unit and axis the E^{0 b}_t table; then, unit by
+// unit, all threads split (1) the Hermite tetrahedron R_{tuv} (closed form),
+// (2) the ket contraction X[h][k], (3) the bra contraction into accumulators
+// held in registers (kGenAcc per thread).
 //
-// raw_kernel: one CTA per (bra group, ket group, ket-Cartesian chunk); it
-// accumulates the raw Cartesian block
-//   raw[ij][kc] = sum_prims pref * sum_{tuv} E^{ij}_{tuv} sum_s (-1)^{|s|} E^{kc}_s R_{tuv+s}
-// in shared memory (stages: Boys -> R tetrahedron -> ket Hermite X[h][kc] ->
-// bra contraction) and stores it to a scratch buffer
-//   raw[((bra * n_ket + ket) * NIJ + ij) * NKC + kc].
-// Modes: three-centre / two-centre (one-centre bra: LJ = 0 and PA = AB = 0) use
-// the Coulomb prefactor 2 pi^{5/2}/(p q sqrt(p+q)) (MI/three_center.cpp:46-49,
-// MI/two_center.cpp:34-37); point charges use 2 pi / p with zeta = p
-// (MI/nuclear_attraction.cpp:44-45, :69).
+// Spherical kets use only the top Hermite level |s| = l_k: a real solid
+// harmonic is a harmonic polynomial, so its Gaussian's Hermite expansion has
+// no lower terms (Hobson's theorem), and the coefficient of s on that level is
+// the spherical coefficient of the Cartesian component s itself.  Cartesian
+// kets use every level with the one-centre coefficients
+// (c_library/mcmurchie_davidson_E_term.hpp:132-139).
 //
-// transform_kernel: raw Cartesian blocks -> spherical (real solid harmonics)
-// or per-component-normalised Cartesian output, written in the packed layout
-//   out[((bra * n_io * n_jo + I * n_jo + J) * n_ko + K) * n_ket + ket].
+// Prefactors: Coulomb 2 pi^{5/2} / (p q sqrt(p+q)) (MI/three_center.cpp:46-49,
+// MI/two_center.cpp:34-37; erf-attenuated for omega > 0); point charges
+// 2 pi / p with zeta = p (MI/nuclear_attraction.cpp:44-45, :69).
+//
+// Output: the packed layout of the fast kernels, molecule m's block at
+// out_begin[m]:
+//   out[((pair * n_io * n_jo + I * n_jo + J) * n_ko + K) * n_aux_m + aux]
+// (spherical or per-component-normalised Cartesian components).
+//
+// overlap_raw_kernel / transform_kernel: the overlap S (E-only).
 #include <algorithm>
+#include <mutex>
 
 #include "eip_common.cuh"
 #include "eip_internal.h"
@@ -39,21 +62,6 @@ int upload_generic_tables() {
     return e == cudaSuccess ? 0 : (int)e;
 }
 
-__device__ __forceinline__ void herm_decode(int idx, int& t, int& u, int& v) {
-    int N = 0;
-    while (nherm(N) <= idx) N++;
-    int r = idx - nherm(N - 1);
-    // r-th component of order N in x-major descending order
-    int a = N;
-    while (r > N - a) {
-        r -= N - a + 1;
-        a--;
-    }
-    t = a;
-    u = N - a - r;
-    v = N - t - u;
-}
-
 __device__ __forceinline__ void cart_decode(int l, int c, int& x, int& y, int& z) {
     int a = l, r = c;
     while (r > l - a) {
@@ -65,217 +73,465 @@ __device__ __forceinline__ void cart_decode(int l, int c, int& x, int& y, int& z
     z = l - x - y;
 }
 
-__device__ __forceinline__ double rt_one_centre(int k, int s) {
-    if (s < 0 || s > k || ((k - s) & 1)) return 0.0;
-    int h = (k - s) / 2;
-    double r = 1.0;
-    for (int i = 2; i <= k; i++) r *= i;
-    for (int i = 2; i <= h; i++) r /= i;
-    for (int i = 2; i <= s; i++) r /= i;
-    for (int i = 0; i < h; i++) r *= 0.5;
-    return r;
+// Index of (x, y, z) among the Cartesian components of l = x + y + z.
+__host__ __device__ __forceinline__ int cart_index(int x, int y, int z) {
+    const int l = x + y + z;
+    return (l - x) * (l - x + 1) / 2 + z;
 }
 
-__device__ __forceinline__ double rt_hermite_r(int t, int m) {
-    if (m < (t + 1) / 2 || m > t) return 0.0;
-    double r = 1.0;
-    for (int i = 2; i <= t; i++) r *= i;
-    for (int i = 2; i <= 2 * m - t; i++) r /= i;
-    for (int i = 2; i <= t - m; i++) r /= i;
-    for (int i = 0; i < t - m; i++) r *= 0.5;
-    return r;
+// Hermite index of (t, u, v) in the order-major tetrahedron (herm_index, run time).
+__device__ __forceinline__ int herm_idx(int t, int u, int v) {
+    const int N = t + u + v;
+    return N * (N + 1) * (N + 2) / 6 + cart_index(t, u, v);
 }
 
 constexpr int kGenThreads = 128;
+constexpr int kGenAcc = 16;   // bra accumulators per thread
+constexpr int kGenUB = 4;     // units per block
+constexpr int kGenMaxL = 21;  // 6 + 6 + 9
+constexpr size_t kGenMaxSmem = 200 * 1024;
 
-struct GenericShape {
-    int LI, LJ, LK, L, LIJ;
-    int NI, NJ, NIJ, NKC, NR, NHB, NE, kc_chunk;
+// Shape of one class for the general kernel, computed on the host.
+struct GenShape {
+    int li, lj, lk, lij, L;
+    int point, spherical;
+    int nbase;      // (0, b) functions, l_j <= |b| <= l_i + l_j
+    int nhb;        // bra Hermite entries, t + u + v <= l_i + l_j
+    int n_io, n_jo, n_ko;
+    int nkc;        // Cartesian components of l_k
+    int ko_chunk, n_chunks;
+    int nea;        // E^{0 b}_t entries per axis, b <= l_i + l_j
+    int rmin;       // lowest Hermite order of R the ket reads
+    int nr;         // nherm(L)
+    int unit_dbl;   // doubles per unit record
+    int maxlev;     // largest transfer level (doubles, one ket component)
+    // shared-memory offsets, in doubles
+    int o_unit, o_hr, o_ket, o_dec, o_work, o_x, o_base, o_lev;
+    int smem_dbl;
 };
 
-__host__ __device__ inline GenericShape generic_shape(int li, int lj, int lk, int kc_chunk) {
-    GenericShape g;
-    g.LI = li; g.LJ = lj; g.LK = lk; g.L = li + lj + lk; g.LIJ = li + lj;
-    g.NI = ncart(li); g.NJ = ncart(lj); g.NIJ = g.NI * g.NJ; g.NKC = ncart(lk);
-    g.NR = nherm(g.L); g.NHB = nherm(g.LIJ);
-    g.NE = (li + 1) * (lj + 1) * (li + lj + 1);
-    g.kc_chunk = kc_chunk;
+// Unit record: [0, L] R^{(m)}_000 (-2 zeta)^m; L+1 prefactor; then X, Y, Z
+// powers (L+1 each); then E^{0 b}_t for x, y, z (nea each); then, Cartesian
+// kets only, the signed one-centre coefficients (l_k+1)^2.
+__host__ __device__ inline int unit_pow(const GenShape& g) { return g.L + 2; }
+__host__ __device__ inline int unit_e(const GenShape& g) { return g.L + 2 + 3 * (g.L + 1); }
+__host__ __device__ inline int unit_ek(const GenShape& g) { return unit_e(g) + 3 * g.nea; }
+
+static GenShape general_shape(int li, int lj, int lk, bool point, bool spherical) {
+    GenShape g{};
+    g.li = li; g.lj = lj; g.lk = point ? 0 : lk; g.lij = li + lj; g.L = g.lij + g.lk;
+    g.point = point; g.spherical = spherical;
+    g.nbase = nherm(g.lij) - nherm(lj - 1);
+    g.nhb = nherm(g.lij);
+    g.n_io = spherical ? nsph(li) : ncart(li);
+    g.n_jo = spherical ? nsph(lj) : ncart(lj);
+    g.n_ko = point ? 1 : (spherical ? nsph(g.lk) : ncart(g.lk));
+    g.nkc = ncart(g.lk);
+    g.ko_chunk = std::max(1, std::min(g.n_ko, kGenThreads * kGenAcc / g.nbase));
+    g.n_chunks = (g.n_ko + g.ko_chunk - 1) / g.ko_chunk;
+    g.nea = (g.lij + 1) * (g.lij + 2) / 2;
+    g.rmin = (spherical && !point) ? g.lk : 0;
+    g.nr = nherm(g.L);
+    g.unit_dbl = unit_ek(g) + ((!spherical && !point) ? (g.lk + 1) * (g.lk + 1) : 0);
+    g.maxlev = 0;
+    for (int k = 1; k <= li; k++) g.maxlev = std::max(g.maxlev, ncart(k) * (nherm(g.lij - k) - nherm(lj - 1)));
+    // layout: unit block | closed-form coefficients | ket rows | tetrahedron
+    // decode (ints) | work region: [R | X] during the unit loop, [base | two
+    // transfer levels] in the epilogue
+    int o = 0;
+    g.o_unit = o; o += kGenUB * g.unit_dbl;
+    g.o_hr = o; o += (kGenMaxL + 1) * (kGenMaxL + 1);
+    g.o_ket = o; o += g.n_ko * g.nkc;
+    g.o_dec = o; o += (g.nr + 1) / 2;
+    g.o_work = o;
+    g.o_x = o + g.nr;
+    g.o_base = o;
+    g.o_lev = o + g.nbase * g.ko_chunk;
+    const int loop_end = g.o_x + g.nhb * g.ko_chunk;
+    const int epi_end = g.o_lev + 2 * g.maxlev;
+    g.smem_dbl = std::max(loop_end, epi_end);
     return g;
 }
 
-size_t generic_smem_bytes(int li, int lj, int lk, int kc_chunk) {
-    GenericShape g = generic_shape(li, lj, lk, kc_chunk);
-    size_t n = g.NR + (g.L + 1) + 8 + 3 * g.NE + (g.LK + 1) * (g.LK + 1) + (size_t)g.NHB * kc_chunk +
-               (size_t)g.NIJ * kc_chunk;
-    return n * sizeof(double);
-}
-
-// mode: 0 Coulomb (three-centre or two-centre), 1 point charges.
 __global__ void __launch_bounds__(kGenThreads)
-raw_kernel(const double* __restrict__ boys_table, int mode, int li, int lj, int lk, int kc_chunk, BraTable bra,
-           KetTable ket, double omega, int skip_lower, double* __restrict__ raw) {
-    extern __shared__ double sm[];
-    const GenericShape g = generic_shape(li, lj, lk, kc_chunk);
-    const int ib = blockIdx.x, ik = blockIdx.y, chunk = blockIdx.z;
-    const int kc0 = chunk * kc_chunk;
-    const int nkc = min(kc_chunk, g.NKC - kc0);
-    if (skip_lower && bra.grp_ao[ib].x > ket.grp_start[ik]) return;
-
-    double* sR = sm;
-    double* sRm = sR + g.NR;
-    double* sPar = sRm + g.L + 1;  // [0] pref
-    double* sE = sPar + 8;         // 3 * NE, index (i*(LJ+1)+j)*(LIJ+1)+t
-    double* sEk = sE + 3 * g.NE;   // (LK+1)^2: E^{k}_s(q)
-    double* sX = sEk + (g.LK + 1) * (g.LK + 1);
-    double* sJ = sX + (size_t)g.NHB * kc_chunk;
+general_kernel(const double* __restrict__ boys_table, GenShape g, BraTable bra, KetTable ket, BatchMap map,
+               double omega, double* __restrict__ out, int* __restrict__ work_counter, int total_items) {
+    extern __shared__ __align__(16) double gsm[];
+    double* sUnit = gsm + g.o_unit;
+    double* sHR = gsm + g.o_hr;
+    double* sKet = gsm + g.o_ket;
+    int* sDec = reinterpret_cast<int*>(gsm + g.o_dec);
+    double* sR = gsm + g.o_work;
+    double* sX = gsm + g.o_x;
+    double* sBase = gsm + g.o_base;
+    double* sLev = gsm + g.o_lev;
+    __shared__ int s_item;
     const int tid = threadIdx.x;
-    for (int e = tid; e < g.NIJ * kc_chunk; e += kGenThreads) sJ[e] = 0.0;
+    // work_counter[0]: next item; work_counter[1]: status (0 ok, else the first
+    // failed self-check: 1 loop bound, 2 molecule/pair/auxiliary index, 3 count)
+    int* status = work_counter + 1;
 
-    const int pb = bra.grp_begin[ib], pe = bra.grp_begin[ib + 1];
-    const int kb = ket.grp_begin[ik], ke = ket.grp_begin[ik + 1];
-    const double4 AB = bra.grp_AB[ib];
-    for (int pp = pb; pp < pe; pp++) {
-        const double4 P = bra.prim_P[pp];
-        const double4 PA = bra.prim_PA[pp];
-        const double p = P.w;
-        for (int kp = kb; kp < ke; kp++) {
-            __syncthreads();
-            const double4 Cq = ket.prim_C[kp];
-            if (tid == 0) {
-                const double X = P.x - Cq.x, Y = P.y - Cq.y, Z = P.z - Cq.z;
-                double zeta, pref;
-                if (mode == 0) {
-                    const double q = Cq.w;
-                    if (omega == 0.0) {
-                        zeta = p * q / (p + q);
-                        pref = PA.w * ket.prim_coef[kp] * kTwoPi52 / (p * q * sqrt(p + q));
+    // per-CTA tables: closed-form Hermite coefficients, spherical ket rows,
+    // tetrahedron decode (t | u << 8 | v << 16)
+    for (int e = tid; e < (kGenMaxL + 1) * (kGenMaxL + 1); e += kGenThreads) {
+        const int t = e / (kGenMaxL + 1), m = e % (kGenMaxL + 1);
+        double r = 0.0;
+        if (m >= (t + 1) / 2 && m <= t) {
+            r = 1.0;
+            for (int i = 2; i <= t; i++) r *= i;
+            for (int i = 2; i <= 2 * m - t; i++) r /= i;
+            for (int i = 2; i <= t - m; i++) r /= i;
+            for (int i = 0; i < t - m; i++) r *= 0.5;
+        }
+        sHR[e] = r;
+    }
+    if (g.spherical && !g.point)
+        for (int e = tid; e < g.n_ko * g.nkc; e += kGenThreads) sKet[e] = c_sph_coef[c_sph_offset[g.lk] + e];
+    for (int N = 0; N <= g.L; N++)
+        for (int c = tid; c < ncart(N); c += kGenThreads) {
+            int x, y, z;
+            cart_decode(N, c, x, y, z);
+            sDec[nherm(N - 1) + c] = x | (y << 8) | (z << 16);
+        }
+    // accumulator entry e = tid + kGenThreads * k holds (base function b, ket component)
+    const int n_ent = g.nbase * g.ko_chunk;
+
+    for (int iter = 0;; iter++) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(work_counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= total_items || item < 0) return;
+        if (iter > total_items) {  // a CTA can never take more items than exist
+            if (tid == 0) atomicCAS(status, 0, 1);
+            return;
+        }
+        int lo = 0, hi = map.n_mol - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(map.item_begin + mid) <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const int m = lo;
+        const int aux0 = __ldg(map.aux_begin + m);
+        const int n_aux = map.aux_count ? __ldg(map.aux_count + m) : __ldg(map.aux_begin + m + 1) - aux0;
+        const int local = item - __ldg(map.item_begin + m);
+        const int chunk = local % g.n_chunks;
+        const int rest = local / g.n_chunks;
+        const int a_local = n_aux > 0 ? rest % n_aux : 0;
+        const int sp_k = n_aux > 0 ? rest / n_aux : 0;
+        const int sp = __ldg(map.sp_begin + m) + sp_k;
+        const int a = aux0 + a_local;
+        // every value tested here is the same for all threads of the CTA
+        if (n_aux <= 0 || sp < 0 || sp >= bra.n_group || sp >= __ldg(map.sp_begin + m + 1) || a < 0 ||
+            a >= ket.n_group) {
+            if (tid == 0) atomicCAS(status, 0, 2);
+            continue;
+        }
+        const int pb = __ldg(bra.grp_begin + sp), pe = __ldg(bra.grp_begin + sp + 1);
+        const int kb = __ldg(ket.grp_begin + a), ke = __ldg(ket.grp_begin + a + 1);
+        const int npp = pe - pb, nkp = ke - kb;
+        if (npp < 0 || npp > 4096 || nkp < 0 || nkp > 4096) {
+            if (tid == 0) atomicCAS(status, 0, 3);
+            continue;
+        }
+        const double4 AB = bra.grp_AB[sp];
+        const int ko0 = chunk * g.ko_chunk;
+        const int nkoc = min(g.ko_chunk, g.n_ko - ko0);
+
+        double acc[kGenAcc];
+#pragma unroll
+        for (int k = 0; k < kGenAcc; k++) acc[k] = 0.0;
+
+        const int n_units = npp * nkp;
+        for (int u0 = 0; u0 < n_units; u0 += kGenUB) {
+            const int nb = min(kGenUB, n_units - u0);
+            __syncthreads();  // the previous block's unit records are no longer read
+            // (A) per unit: prefactor, Boys, R^{(m)}_000, powers; per unit and axis: E^{0 b}_t
+            for (int w = tid; w < 4 * nb; w += kGenThreads) {
+                const int ub = w < nb ? w : (w - nb) / 3;
+                const int u = u0 + ub;
+                const int pp = pb + u / nkp, kp = kb + u % nkp;
+                double* U = sUnit + ub * g.unit_dbl;
+                const double4 P = bra.prim_P[pp];
+                if (w < nb) {
+                    const double4 PA = bra.prim_PA[pp];
+                    const double4 Cq = ket.prim_C[kp];
+                    const double c = PA.w * ket.prim_coef[kp];
+                    const double p = P.w, q = Cq.w;
+                    double zeta, pref;
+                    if (g.point) {
+                        if (omega == 0.0) {
+                            zeta = p;
+                            pref = c * 2.0 * kPi / p;
+                        } else {
+                            zeta = p * omega * omega / (p + omega * omega);
+                            pref = c * 2.0 * kPi * omega / (p * sqrt(p + omega * omega));
+                        }
                     } else {
-                        zeta = 1.0 / (1.0 / p + 1.0 / q + 1.0 / (omega * omega));
-                        pref = PA.w * ket.prim_coef[kp] * kTwoPi52 * omega /
-                               (p * q * sqrt(p * q + (p + q) * omega * omega));
+                        if (omega == 0.0) {
+                            zeta = p * q / (p + q);
+                            pref = c * kTwoPi52 / (p * q * sqrt(p + q));
+                        } else {
+                            zeta = 1.0 / (1.0 / p + 1.0 / q + 1.0 / (omega * omega));
+                            pref = c * kTwoPi52 * omega / (p * q * sqrt(p * q + (p + q) * omega * omega));
+                        }
+                    }
+                    const double X = P.x - Cq.x, Y = P.y - Cq.y, Z = P.z - Cq.z;
+                    double F[kMaxBoysM + 1];
+                    boys_rt(boys_table, g.L, zeta * (X * X + Y * Y + Z * Z), F);
+                    double f = 1.0;
+                    for (int mm = 0; mm <= g.L; mm++) {
+                        U[mm] = F[mm] * f;
+                        f *= -2.0 * zeta;
+                    }
+                    if (g.spherical && !g.point) {
+                        // top Hermite level only: weight (-1/(2q))^{l_k}
+                        const double w2q = -0.5 / q;
+                        for (int i = 0; i < g.lk; i++) pref *= w2q;
+                    } else if (!g.point) {
+                        // signed one-centre coefficients (-1)^s E^{k,0}_s(q)
+                        double* ek = U + unit_ek(g);
+                        const double inv2q = 0.5 / q;
+                        for (int k = 0; k <= g.lk; k++)
+                            for (int s = 0; s <= g.lk; s++) {
+                                double cf = 0.0;
+                                if (s <= k && !((k - s) & 1)) {
+                                    const int h = (k - s) / 2;
+                                    cf = 1.0;
+                                    for (int i = 2; i <= k; i++) cf *= i;
+                                    for (int i = 2; i <= h; i++) cf /= i;
+                                    for (int i = 2; i <= s; i++) cf /= i;
+                                    for (int i = 0; i < h; i++) cf *= 0.5;
+                                    for (int i = 0; i < (k + s) / 2; i++) cf *= inv2q;
+                                    if (s & 1) cf = -cf;
+                                }
+                                ek[k * (g.lk + 1) + s] = cf;
+                            }
+                    }
+                    U[g.L + 1] = pref;
+                    double* pw = U + unit_pow(g);
+                    double px = 1.0, py = 1.0, pz = 1.0;
+                    for (int k = 0; k <= g.L; k++) {
+                        pw[k] = px;
+                        pw[g.L + 1 + k] = py;
+                        pw[2 * (g.L + 1) + k] = pz;
+                        px *= X;
+                        py *= Y;
+                        pz *= Z;
                     }
                 } else {
-                    if (omega == 0.0) {
-                        zeta = p;
-                        pref = PA.w * ket.prim_coef[kp] * 2.0 * kPi / p;
+                    // E^{0,b+1}_t = E^{0,b}_{t-1} / (2p) + PB E^{0,b}_t + (t+1) E^{0,b}_{t+1}, PB = PA + AB
+                    const int d = (w - nb) % 3;
+                    const double4 PA = bra.prim_PA[pp];
+                    const double pb_d = d == 0 ? PA.x + AB.x : (d == 1 ? PA.y + AB.y : PA.z + AB.z);
+                    const double inv2p = 0.5 / P.w;
+                    double* E = U + unit_e(g) + d * g.nea;
+                    E[0] = 1.0;
+                    for (int b = 0; b < g.lij; b++) {
+                        const double* Eb = E + b * (b + 1) / 2;
+                        double* En = E + (b + 1) * (b + 2) / 2;
+                        for (int t = 0; t <= b + 1; t++) {
+                            double v = 0.0;
+                            if (t >= 1) v = inv2p * Eb[t - 1];
+                            if (t <= b) v = fma(pb_d, Eb[t], v);
+                            if (t + 1 <= b) v = fma((double)(t + 1), Eb[t + 1], v);
+                            En[t] = v;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            for (int ub = 0; ub < nb; ub++) {
+                const double* U = sUnit + ub * g.unit_dbl;
+                // (1) tetrahedron entries of order >= rmin, closed form
+                // (c_library/mcmurchie_davidson_R_term.hpp:31-37)
+                {
+                    const double* Rm = U;
+                    const double* px = U + unit_pow(g);
+                    const double* py = px + g.L + 1;
+                    const double* pz = py + g.L + 1;
+                    for (int idx = nherm(g.rmin - 1) + tid; idx < g.nr; idx += kGenThreads) {
+                        const int dc = sDec[idx];
+                        const int t = dc & 255, u = (dc >> 8) & 255, v = dc >> 16;
+                        double r = 0.0;
+                        for (int mx = (t + 1) / 2; mx <= t; mx++) {
+                            double ry = 0.0;
+                            for (int my = (u + 1) / 2; my <= u; my++) {
+                                double rz = 0.0;
+                                for (int mz = (v + 1) / 2; mz <= v; mz++)
+                                    rz = fma(sHR[v * (kGenMaxL + 1) + mz] * pz[2 * mz - v], Rm[mx + my + mz], rz);
+                                ry = fma(sHR[u * (kGenMaxL + 1) + my] * py[2 * my - u], rz, ry);
+                            }
+                            r = fma(sHR[t * (kGenMaxL + 1) + mx] * px[2 * mx - t], ry, r);
+                        }
+                        sR[idx] = r;
+                    }
+                }
+                __syncthreads();
+                // (2) ket: X[h][k] for the chunk's ket components
+                for (int e = tid; e < g.nhb * nkoc; e += kGenThreads) {
+                    const int h = e / nkoc, kl = e - h * nkoc, ko = ko0 + kl;
+                    const int dh = sDec[h];
+                    const int t = dh & 255, u = (dh >> 8) & 255, v = dh >> 16;
+                    double x = 0.0;
+                    if (g.point) {
+                        x = sR[h];
+                    } else if (g.spherical) {
+                        const double* row = sKet + ko * g.nkc;
+                        const int first = nherm(g.lk - 1);
+                        for (int c = 0; c < g.nkc; c++) {
+                            const double w = row[c];
+                            if (w == 0.0) continue;
+                            const int dc = sDec[first + c];
+                            x = fma(w, sR[herm_idx(t + (dc & 255), u + ((dc >> 8) & 255), v + (dc >> 16))], x);
+                        }
                     } else {
-                        zeta = p * omega * omega / (p + omega * omega);
-                        pref = PA.w * ket.prim_coef[kp] * 2.0 * kPi * omega / (p * sqrt(p + omega * omega));
+                        int kx, ky, kz;
+                        cart_decode(g.lk, ko, kx, ky, kz);
+                        const double* ek = U + unit_ek(g);
+                        const int w1 = g.lk + 1;
+                        for (int sx = kx & 1; sx <= kx; sx += 2)
+                            for (int sy = ky & 1; sy <= ky; sy += 2) {
+                                const double exy = ek[kx * w1 + sx] * ek[ky * w1 + sy];
+                                for (int sz = kz & 1; sz <= kz; sz += 2)
+                                    x = fma(exy * ek[kz * w1 + sz], sR[herm_idx(t + sx, u + sy, v + sz)], x);
+                            }
                     }
+                    sX[e] = x;
                 }
-                double F[kMaxBoysM + 1];
-                boys_rt(boys_table, g.L, zeta * (X * X + Y * Y + Z * Z), F);
-                double f = 1.0;
-                for (int m = 0; m <= g.L; m++) {
-                    sRm[m] = f * F[m];
-                    f *= -2.0 * zeta;
-                }
-                sPar[0] = pref;
-                sPar[1] = X; sPar[2] = Y; sPar[3] = Z;
-            } else if (tid >= 32 && tid < 35) {
-                const int d = tid - 32;
-                const double pa = d == 0 ? PA.x : (d == 1 ? PA.y : PA.z);
-                const double ab = d == 0 ? AB.x : (d == 1 ? AB.y : AB.z);
-                const double inv2p = 0.5 / p;
-                const int N = g.LIJ;
-                double W[13][7][13];  // i <= 12, j <= 6, t <= 12
-                for (int i = 0; i <= N; i++)
-                    for (int j = 0; j <= g.LJ; j++)
-                        for (int t = 0; t <= N; t++) W[i][j][t] = 0.0;
-                W[0][0][0] = 1.0;
-                for (int i = 0; i < N; i++)
-                    for (int t = 0; t <= i + 1; t++) {
-                        double v = 0.0;
-                        if (t >= 1) v = inv2p * W[i][0][t - 1];
-                        if (t <= i) v = fma(pa, W[i][0][t], v);
-                        if (t + 1 <= i) v = fma((double)(t + 1), W[i][0][t + 1], v);
-                        W[i + 1][0][t] = v;
-                    }
-                for (int j = 0; j < g.LJ; j++)
-                    for (int i = 0; i + j + 1 <= N; i++)
-                        for (int t = 0; t <= i + j + 1; t++) W[i][j + 1][t] = fma(ab, W[i][j][t], W[i + 1][j][t]);
-                double* out = sE + d * g.NE;
-                for (int i = 0; i <= g.LI; i++)
-                    for (int j = 0; j <= g.LJ; j++)
-                        for (int t = 0; t <= N; t++) out[(i * (g.LJ + 1) + j) * (N + 1) + t] = W[i][j][t];
-            } else if (tid == 64) {
-                const double inv2q = mode == 0 ? 0.5 / Cq.w : 0.0;
-                for (int k = 0; k <= g.LK; k++)
-                    for (int s = 0; s <= g.LK; s++) {
-                        double c = rt_one_centre(k, s);
-                        for (int i = 0; i < (k + s) / 2; i++) c *= inv2q;
-                        sEk[k * (g.LK + 1) + s] = c;
-                    }
-            }
-            __syncthreads();
-            {
-                const double X = sPar[1], Y = sPar[2], Z = sPar[3];
-                for (int idx = tid; idx < g.NR; idx += kGenThreads) {
-                    int t, u, v;
-                    herm_decode(idx, t, u, v);
-                    double r = 0.0;
-                    for (int mx = (t + 1) / 2; mx <= t; mx++) {
-                        double ry = 0.0;
-                        for (int my = (u + 1) / 2; my <= u; my++) {
-                            double rz = 0.0;
-                            for (int mz = (v + 1) / 2; mz <= v; mz++)
-                                rz = fma(rt_hermite_r(v, mz) * pow(Z, (double)(2 * mz - v)), sRm[mx + my + mz], rz);
-                            ry = fma(rt_hermite_r(u, my) * pow(Y, (double)(2 * my - u)), rz, ry);
+                __syncthreads();
+                // (3) bra: acc[(b, k)] += pref sum_t Ex sum_u Ey sum_v Ez X[tuv][k]
+                {
+                    const double pref = U[g.L + 1];
+                    const double* Ex = U + unit_e(g);
+                    const double* Ey = Ex + g.nea;
+                    const double* Ez = Ey + g.nea;
+#pragma unroll
+                    for (int k = 0; k < kGenAcc; k++) {
+                        const int e = tid + kGenThreads * k;
+                        if (e < n_ent) {
+                            const int b = e / g.ko_chunk, kl = e - b * g.ko_chunk;
+                            if (kl < nkoc) {
+                                const int db = sDec[nherm(g.lj - 1) + b];
+                                const int bx = db & 255, by = (db >> 8) & 255, bz = db >> 16;
+                                const double* ex = Ex + bx * (bx + 1) / 2;
+                                const double* ey = Ey + by * (by + 1) / 2;
+                                const double* ez = Ez + bz * (bz + 1) / 2;
+                                double s = 0.0;
+                                for (int t = 0; t <= bx; t++) {
+                                    double su = 0.0;
+                                    for (int u = 0; u <= by; u++) {
+                                        double sv = 0.0;
+                                        for (int v = 0; v <= bz; v++)
+                                            sv = fma(ez[v], sX[herm_idx(t, u, v) * nkoc + kl], sv);
+                                        su = fma(ey[u], sv, su);
+                                    }
+                                    s = fma(ex[t], su, s);
+                                }
+                                acc[k] = fma(pref, s, acc[k]);
+                            }
                         }
-                        r = fma(rt_hermite_r(t, mx) * pow(X, (double)(2 * mx - t)), ry, r);
                     }
-                    sR[idx] = r;
                 }
-            }
-            __syncthreads();
-            for (int e = tid; e < g.NHB * nkc; e += kGenThreads) {
-                const int h = e / nkc, c = e - h * nkc;
-                int t, u, v, kx, ky, kz;
-                herm_decode(h, t, u, v);
-                cart_decode(g.LK, kc0 + c, kx, ky, kz);
-                double x = 0.0;
-                for (int sx = kx & 1; sx <= kx; sx += 2)
-                    for (int sy = ky & 1; sy <= ky; sy += 2)
-                        for (int sz = kz & 1; sz <= kz; sz += 2) {
-                            const double ek = sEk[kx * (g.LK + 1) + sx] * sEk[ky * (g.LK + 1) + sy] *
-                                              sEk[kz * (g.LK + 1) + sz];
-                            const double r = sR[herm_index(t + sx, u + sy, v + sz)];
-                            x = ((sx + sy + sz) & 1) ? fma(-ek, r, x) : fma(ek, r, x);
-                        }
-                sX[h * kc_chunk + c] = x;
-            }
-            __syncthreads();
-            const double pref = sPar[0];
-            const int N1 = g.LIJ + 1;
-            for (int e = tid; e < g.NIJ * nkc; e += kGenThreads) {
-                const int ij = e / nkc, c = e - ij * nkc;
-                const int ci = ij / g.NJ, cj = ij - ci * g.NJ;
-                int ix, iy, iz, jx, jy, jz;
-                cart_decode(g.LI, ci, ix, iy, iz);
-                cart_decode(g.LJ, cj, jx, jy, jz);
-                const double* ex = sE + (ix * (g.LJ + 1) + jx) * N1;
-                const double* ey = sE + g.NE + (iy * (g.LJ + 1) + jy) * N1;
-                const double* ez = sE + 2 * g.NE + (iz * (g.LJ + 1) + jz) * N1;
-                double s = 0.0;
-                for (int t = 0; t <= ix + jx; t++) {
-                    double su = 0.0;
-                    for (int u = 0; u <= iy + jy; u++) {
-                        double sv = 0.0;
-                        for (int v = 0; v <= iz + jz; v++) sv = fma(ez[v], sX[herm_index(t, u, v) * kc_chunk + c], sv);
-                        su = fma(ey[u], sv, su);
-                    }
-                    s = fma(ex[t], su, s);
-                }
-                sJ[ij * kc_chunk + c] = fma(pref, s, sJ[ij * kc_chunk + c]);
             }
         }
+        __syncthreads();
+        // Epilogue: base integrals to shared memory, transfer l_i onto centre A,
+        // bra (and, Cartesian, ket) output transform, stores.
+#pragma unroll
+        for (int k = 0; k < kGenAcc; k++) {
+            const int e = tid + kGenThreads * k;
+            if (e < n_ent) sBase[e] = acc[k];
+        }
+        __syncthreads();
+        const double ab[3] = {AB.x, AB.y, AB.z};
+        const size_t obase = (size_t)__ldg(map.out_begin + m);
+        double wsum = 0.0;  // this thread's stored values (optional per-molecule checksum)
+        for (int kl = 0; kl < nkoc; kl++) {
+            // level k holds (a, b) for |a| = k and b the first nb_k base functions
+            const double* src = sBase + kl;
+            int src_stride = g.ko_chunk;  // level 0: column kl of the base block
+            int nb_prev = g.nbase;
+            for (int k = 1; k <= g.li; k++) {
+                const int nbk = nherm(g.lij - k) - nherm(g.lj - 1);
+                double* dst = sLev + ((k & 1) ? 0 : g.maxlev);
+                for (int e = tid; e < ncart(k) * nbk; e += kGenThreads) {
+                    const int ai = e / nbk, bi = e - ai * nbk;
+                    int ax, ay, az;
+                    cart_decode(k, ai, ax, ay, az);
+                    const int d = ax > 0 ? 0 : (ay > 0 ? 1 : 2);
+                    if (d == 0) ax--;
+                    else if (d == 1) ay--;
+                    else az--;
+                    const int ap = cart_index(ax, ay, az);
+                    const int db = sDec[nherm(g.lj - 1) + bi];
+                    int bx = db & 255, by = (db >> 8) & 255, bz = db >> 16;
+                    if (d == 0) bx++;
+                    else if (d == 1) by++;
+                    else bz++;
+                    const int bn = nherm(bx + by + bz - 1) - nherm(g.lj - 1) + cart_index(bx, by, bz);
+                    dst[e] = src[(ap * nb_prev + bn) * src_stride] - ab[d] * src[(ap * nb_prev + bi) * src_stride];
+                }
+                __syncthreads();
+                src = dst;
+                src_stride = 1;
+                nb_prev = nbk;
+            }
+            // final level: (a, b) with |a| = l_i, |b| = l_j (b index < ncart(l_j))
+            const int ko = ko0 + kl;
+            const double knorm = (g.spherical || g.point) ? 1.0 : c_cart_norm[c_cart_norm_offset[g.lk] + ko];
+            for (int e = tid; e < g.n_io * g.n_jo; e += kGenThreads) {
+                const int I = e / g.n_jo, J = e - I * g.n_jo;
+                double v = 0.0;
+                for (int ca = 0; ca < ncart(g.li); ca++) {
+                    const double wi = g.spherical ? c_sph_coef[c_sph_offset[g.li] + I * ncart(g.li) + ca]
+                                                  : (I == ca ? c_cart_norm[c_cart_norm_offset[g.li] + ca] : 0.0);
+                    if (wi == 0.0) continue;
+                    double vj = 0.0;
+                    for (int cb = 0; cb < ncart(g.lj); cb++) {
+                        const double wj = g.spherical ? c_sph_coef[c_sph_offset[g.lj] + J * ncart(g.lj) + cb]
+                                                      : (J == cb ? c_cart_norm[c_cart_norm_offset[g.lj] + cb] : 0.0);
+                        if (wj != 0.0) vj = fma(wj, src[(ca * nb_prev + cb) * src_stride], vj);
+                    }
+                    v = fma(wi, vj, v);
+                }
+                const size_t row = (((size_t)sp_k * g.n_io + I) * g.n_jo + J) * g.n_ko + ko;
+                out[obase + row * n_aux + a_local] = v * knorm;
+                wsum += v * knorm;
+            }
+            __syncthreads();
+        }
+        if (map.checksum && wsum != 0.0) atomicAdd(map.checksum + m, wsum);
     }
-    __syncthreads();
-    const size_t base = ((size_t)ib * ket.n_group + ik) * g.NIJ;
-    for (int e = tid; e < g.NIJ * nkc; e += kGenThreads) {
-        const int ij = e / nkc, c = e - ij * nkc;
-        raw[(base + ij) * g.NKC + kc0 + c] = sJ[ij * kc_chunk + c];
-    }
+}
+
+int general_chunks(int li, int lj, int lk, bool point, bool spherical) {
+    return general_shape(li, lj, lk, point, spherical).n_chunks;
+}
+
+int launch_general(int li, int lj, int lk, bool point, bool spherical, const BraTable& bra, const KetTable& ket,
+                   const BatchMap& map, int total_items, double omega, double* out, int* counter, cudaStream_t s) {
+    if (li < 0 || li > lj || lj > kMaxAuxL || lk < 0 || lk > kMaxAuxL || li + lj + (point ? 0 : lk) > kGenMaxL)
+        return 1;
+    if (total_items <= 0) return 0;
+    const GenShape g = general_shape(li, lj, lk, point, spherical);
+    const size_t smem = sizeof(double) * (size_t)g.smem_dbl;
+    if (smem > kGenMaxSmem) return 3;
+    const double* table = boys_table_device();
+    if (!table) return 2;
+    // the shared-memory limit is raised once per device to the most any class takes
+    static std::atomic<int> configured[kMaxDevices];
+    if (persistent_grid(reinterpret_cast<const void*>(general_kernel), kGenThreads, kGenMaxSmem, configured) <= 0)
+        return 2;
+    int per_sm = 0, sms = 0;
+    const int dev = current_device();
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, general_kernel, kGenThreads, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 2;
+    const int grid = std::min(total_items, std::max(1, per_sm) * sms);
+    general_kernel<<<grid, kGenThreads, smem, s>>>(table, g, bra, ket, map, omega, out, counter, total_items);
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
 // Overlap: one thread per (shell pair, ci, cj) raw Cartesian element;
@@ -365,43 +621,6 @@ __global__ void transform_kernel(int li, int lj, int lk, bool spherical, int n_b
         }
         out[e] = v;
     }
-}
-
-int generic_kc_chunk(int li, int lj, int lk) {
-    const int NKC = ncart(lk), NIJ = ncart(li) * ncart(lj), NHB = nherm(li + lj);
-    int chunk = NKC;
-    while (chunk > 1 && (size_t)(NIJ + NHB) * chunk > 12000) chunk = (chunk + 1) / 2;
-    return chunk;
-}
-
-// Largest dynamic shared memory raw_kernel takes over every class the C ABI
-// accepts (orbital l <= 6, auxiliary l <= 9; the two-centre bra up to l = 9).
-static size_t generic_max_smem() {
-    size_t m = 0;
-    for (int li = 0; li <= kMaxAuxL; li++)
-        for (int lj = 0; lj <= kMaxOrbitalL; lj++)
-            for (int lk = 0; lk <= kMaxAuxL; lk++)
-                if (li + lj + lk <= kMaxBoysM) m = std::max(m, generic_smem_bytes(li, lj, lk, generic_kc_chunk(li, lj, lk)));
-    return m;
-}
-
-int launch_generic_raw(int mode, int li, int lj, int lk, const BraTable& bra, const KetTable& ket, double omega,
-                       int skip_lower, double* raw, cudaStream_t s) {
-    if (bra.n_group == 0 || ket.n_group == 0) return 0;
-    const int chunk = generic_kc_chunk(li, lj, lk);
-    const int n_chunks = (ncart(lk) + chunk - 1) / chunk;
-    const size_t smem = generic_smem_bytes(li, lj, lk, chunk);
-    // the shared-memory limit is raised once per device, to the largest class's
-    // need (persistent_grid caches per device and serialises the set-up)
-    static std::atomic<int> configured[kMaxDevices];
-    if (persistent_grid(reinterpret_cast<const void*>(raw_kernel), kGenThreads, generic_max_smem(), configured) <= 0)
-        return 2;
-    const double* table = boys_table_device();
-    if (!table) return 2;
-    if (ket.n_group > 65535) return 3;
-    dim3 grid(bra.n_group, ket.n_group, n_chunks);
-    raw_kernel<<<grid, kGenThreads, smem, s>>>(table, mode, li, lj, lk, chunk, bra, ket, omega, skip_lower, raw);
-    return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
 int launch_overlap_raw(int li, int lj, const BraTable& bra, const double* prim_b, double* raw, cudaStream_t s) {

@@ -13,13 +13,14 @@
 // Working memory: g_noalloc_scratch, kNoAllocScratchBytes = 16 MiB, allocated
 // with the module on every GPU that loads the library and held until the
 // process exits.  A call needs, for its n_pair x n_aux_primitive primitive
-// triplets, the converted input tables plus one raw Cartesian block and one
+// triplets, the converted input tables, a one-molecule work list and one
 // output block per primitive triplet; a call that needs more is rejected with
-// status 4 and a message on stderr, before anything is launched.
+// status 4 (eip_last_error() says why), before anything is launched.
 //
 // Every call on the device shares that array, and the array keeps the last
-// call's contents.  Nothing in it needs to start at zero: each call writes
-// every word it reads.  Two calls whose kernels overlap on the GPU (different
+// call's contents.  The only words that must start at zero, the work counter
+// and status of the integral kernel, are cleared by the call's first kernel;
+// every other word a call reads it has written itself.  Two calls whose kernels overlap on the GPU (different
 // streams, or different host threads, without ordering) race on the array:
 // callers must order them, e.g. issue all calls on one stream.
 //
@@ -58,7 +59,7 @@ size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 // Byte offsets of one call's arrays in the scratch array.
 struct ScratchLayout {
-    size_t bbeg, bao, bab, bp, bpa, kbeg, kst, kc, kco, raw, pk, total;
+    size_t bbeg, bao, bab, bp, bpa, kbeg, kst, kc, kco, misc, pk, total;
 };
 
 ScratchLayout scratch_layout(int i_L, int j_L, int k_L, size_t np, size_t na, bool spherical) {
@@ -75,7 +76,7 @@ ScratchLayout scratch_layout(int i_L, int j_L, int k_L, size_t np, size_t na, bo
     l.kst = off; off += align256(sizeof(int) * na);
     l.kc = off; off += align256(sizeof(double4) * na);
     l.kco = off; off += align256(sizeof(double) * na);
-    l.raw = off; off += align256(sizeof(double) * np * na * ncart(i_L) * ncart(j_L) * ncart(k_L));
+    l.misc = off; off += align256(16 * sizeof(int) + sizeof(long long));
     l.pk = off; off += align256(sizeof(double) * np * na * ni * nj * nk);
     l.total = off;
     return l;
@@ -113,16 +114,24 @@ unsigned char* scratch_on_current_device() {
     return p;
 }
 
-// Reference-format device arrays -> the generic kernel's tables, one group per
-// primitive pair and per auxiliary primitive (no grouping: nothing to sort).
+// Reference-format device arrays -> the general kernel's tables, one group per
+// primitive pair and per auxiliary primitive (no grouping: nothing to sort),
+// and its one-molecule work list: misc[0..3] counter and status (cleared),
+// [4..5] item begin, [6..7] pair begin, [8..9] auxiliary begin; out_begin = 0.
 __global__ void noalloc_tables_kernel(const double* __restrict__ P_p, const double* __restrict__ A_a,
                                       const double* __restrict__ B_b, const double* __restrict__ coef,
                                       const int* __restrict__ ia, const int* __restrict__ ja, int n_pair,
                                       const double* __restrict__ C_q, const double* __restrict__ aux_coef,
                                       const int* __restrict__ aux_start, int n_aux, int* bra_begin, int2* bra_ao,
                                       double4* bra_AB, double4* bra_P, double4* bra_PA, int* ket_begin,
-                                      int* ket_start, double4* ket_C, double* ket_coef) {
+                                      int* ket_start, double4* ket_C, double* ket_coef, int* misc,
+                                      long long* out_begin, int items) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        const int m[10] = {0, 0, 0, 0, 0, items, 0, n_pair, 0, n_aux};
+        for (int k = 0; k < 10; k++) misc[k] = m[k];
+        *out_begin = 0;
+    }
     if (i <= n_pair) bra_begin[i] = i;
     if (i <= n_aux) ket_begin[i] = i;
     if (i < n_pair) {
@@ -218,13 +227,16 @@ extern "C" int eip_three_center_noalloc(const int i_L, const int j_L, const int 
     const ScratchLayout l = scratch_layout(i_L, j_L, k_L, np, na, spherical);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int nmax = (int)std::max(np, na) + 1;
+    const long long items = (long long)np * na * general_chunks(i_L, j_L, k_L, false, spherical);
+    int* misc = reinterpret_cast<int*>(s + l.misc);
+    long long* out_begin = reinterpret_cast<long long*>(s + l.misc + 16 * sizeof(int));
     noalloc_tables_kernel<<<(nmax + 127) / 128, 128, 0, st>>>(
         pair_P_p, pair_A_a, pair_B_b, pair_coefficient, pair_i_ao_start, pair_j_ao_start, n_pair_ij, aux_A_a,
         aux_coefficient, aux_i_aux_start, n_aux_primitive_k, reinterpret_cast<int*>(s + l.bbeg),
         reinterpret_cast<int2*>(s + l.bao), reinterpret_cast<double4*>(s + l.bab),
         reinterpret_cast<double4*>(s + l.bp), reinterpret_cast<double4*>(s + l.bpa),
         reinterpret_cast<int*>(s + l.kbeg), reinterpret_cast<int*>(s + l.kst), reinterpret_cast<double4*>(s + l.kc),
-        reinterpret_cast<double*>(s + l.kco));
+        reinterpret_cast<double*>(s + l.kco), misc, out_begin, (int)items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("eip_three_center_noalloc: table kernel launch", e);
@@ -235,10 +247,9 @@ extern "C" int eip_three_center_noalloc(const int i_L, const int j_L, const int 
                  reinterpret_cast<double4*>(s + l.bpa), nullptr};
     KetTable ket{n_aux_primitive_k, reinterpret_cast<int*>(s + l.kbeg), reinterpret_cast<int*>(s + l.kst),
                  reinterpret_cast<double4*>(s + l.kc), reinterpret_cast<double*>(s + l.kco)};
-    double* raw = reinterpret_cast<double*>(s + l.raw);
     double* packed = reinterpret_cast<double*>(s + l.pk);
-    int rc = launch_generic_raw(0, i_L, j_L, k_L, bra, ket, omega, 0, raw, st);
-    if (rc == 0) rc = launch_transform(i_L, j_L, k_L, spherical, n_pair_ij, n_aux_primitive_k, raw, packed, st);
+    BatchMap map{1, misc + 4, misc + 6, misc + 8, out_begin, nullptr, nullptr, nullptr};
+    int rc = launch_general(i_L, j_L, k_L, false, spherical, bra, ket, map, (int)items, omega, packed, misc, st);
     if (rc == 0) {
         const long long total = (long long)np * ni * nj * nk * na;
         long long blocks = (total + 255) / 256;

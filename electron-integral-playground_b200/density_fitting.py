@@ -9,10 +9,18 @@ from its auxiliary windows and the metric (P|Q):
     J_{mu nu} = sum_P (mu nu|P) c_P
 
 Everything stays on the device: each packed class block [pair shell][I][J][K]
-[aux shell] is read as a (pairs*I*J) x (K*aux) matrix; the density is gathered
-into the block's row order (off-diagonal shell pairs count twice) and the two
-contractions are matrix-vector products (library GEMV), so the dense
+[aux shell] is read as a (pairs*I*J) x (K*aux) matrix, so the dense
 (n_aux, n_ao, n_ao) tensor is never formed.
+
+* ``BatchCoulomb`` (many molecules at once, the whole batch output resident):
+  gamma and J are the library's own kernels (eip_batch_df_gamma /
+  eip_batch_df_coulomb, csrc/df.cu), one launch each for every block of every
+  molecule; the FP64 Cholesky factorisation of each (P|Q) and the triangular
+  solves are library calls (torch.linalg, cuSOLVER).
+* ``coulomb_matrix`` (one molecule, optionally window by window over the
+  auxiliary basis): the density is gathered into each block's row order
+  (off-diagonal shell pairs count twice) and the contractions are library
+  GEMV calls on the window buffer.
 """
 
 import numpy as np
@@ -136,3 +144,46 @@ def coulomb_matrix(molecule, pair_data, aux_data, D, precision="fp64", window_by
     b.status()
     b.close()
     return J, c, gamma
+
+
+class BatchCoulomb:
+    """Density-fitted J for every molecule of a batch with its packed output
+    bound and computed (``batch.run()``):
+
+        gamma = (mu nu|P) D,   c = (P|Q)^{-1} gamma,   J = (mu nu|P) c
+
+    ``metric_factors``: per molecule the lower Cholesky factor of its (P|Q)
+    (device, FP64), e.g. ``torch.linalg.cholesky(metric_matrix(...))``.  The
+    densities and results are concatenated device arrays (molecule m's n_ao^2
+    block after the previous molecules'); ``run`` queues everything on the
+    batch stream's side of the current torch stream and returns J."""
+
+    def __init__(self, torch, batch, metric_factors):
+        self.torch = torch
+        self.batch = batch
+        self.n_ao2, self.n_aux = batch.df_plan()
+        self.factors = list(metric_factors)
+        self.aux_off = np.concatenate([[0], np.cumsum([m.n_aux for m in batch.molecules])]).astype(np.int64)
+        self.ao_off = np.concatenate([[0], np.cumsum([m.n_ao ** 2 for m in batch.molecules])]).astype(np.int64)
+        dev = "cuda"
+        self.gamma = torch.zeros(max(self.n_aux, 1), dtype=torch.float64, device=dev)
+        self.c = torch.zeros(max(self.n_aux, 1), dtype=torch.float64, device=dev)
+        self.J = torch.zeros(max(self.n_ao2, 1), dtype=torch.float64, device=dev)
+        self.stream = torch.cuda.ExternalStream(batch.stream)
+
+    def run(self, D):
+        """D: concatenated densities (device tensor of n_ao2 doubles).  Returns
+        the concatenated J (device tensor; valid once the batch stream is done)."""
+        torch = self.torch
+        self.batch.df_gamma(D.data_ptr(), self.gamma.data_ptr())
+        with torch.cuda.stream(self.stream):
+            for m, Lf in enumerate(self.factors):
+                a0, a1 = int(self.aux_off[m]), int(self.aux_off[m + 1])
+                if a1 > a0:
+                    self.c[a0:a1] = torch.cholesky_solve(self.gamma[a0:a1, None], Lf)[:, 0]
+        self.batch.df_coulomb(self.c.data_ptr(), self.J.data_ptr())
+        return self.J
+
+    def molecule_J(self, m):
+        n = self.batch.molecules[m].n_ao
+        return self.J[int(self.ao_off[m]):int(self.ao_off[m + 1])].view(n, n)

@@ -232,6 +232,20 @@ unsigned long long eip_batch_launches_per_run(eip_batch* batch);
 int eip_batch_checksums(eip_batch* batch, double* host_checksums);
 int eip_batch_copy_output(eip_batch* batch, long long offset, long long count, double* host);
 void* eip_batch_stream(eip_batch* batch);
+/* Density-fitted Coulomb contractions over the batch's packed (mu nu|P)
+ * output, on the batch stream (no counterpart in the reference, whose
+ * consumers read its dense tensor):
+ *   gamma_P   = sum_{mu nu} (mu nu|P) D_{mu nu}
+ *   J_{mu nu} = sum_P (mu nu|P) c_P
+ * for every molecule at once.  df_plan (after build, with the molecules'
+ * n_ao and n_aux) lists the blocks; then, after a run into the bound output,
+ * df_gamma / df_coulomb take DEVICE arrays: D and J hold the molecules'
+ * n_ao x n_ao row-major matrices one after the other, gamma and c their
+ * n_aux vectors.  gamma and J are overwritten.  Point-charge classes are not
+ * part of the contraction. */
+int eip_batch_df_plan(eip_batch* batch, const int* n_ao, const int* n_aux);
+int eip_batch_df_gamma(eip_batch* batch, const double* D, double* gamma);
+int eip_batch_df_coulomb(eip_batch* batch, const double* c, double* J);
 const char* eip_batch_error(eip_batch* batch);
 void eip_batch_destroy(eip_batch* batch);
 

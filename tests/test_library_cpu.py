@@ -121,9 +121,9 @@ def test_noalloc_admission_check_on_host():
     assert limit == 16 << 20
     rc, need = _noalloc_check(L, 1, 2, 3, 20, 30)
     assert rc == 0 and 0 < need <= limit
-    # need grows with the primitive triplets: the class's raw Cartesian plus
-    # spherical block per triplet dominates
-    per = 8 * (3 * 6 * 10 + 3 * 5 * 7)
+    # need grows with the primitive triplets: the class's spherical output
+    # block per triplet dominates
+    per = 8 * 3 * 5 * 7
     assert need >= 20 * 30 * per
     rc, need = _noalloc_check(L, 1, 2, 4, 2000, 3000)
     assert rc == 4 and need > limit
