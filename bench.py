@@ -370,6 +370,108 @@ def run_config2(torch, bt, threshold, seed=0, window_bytes=24e9):
     }
 
 
+def best_of(fn, repeats=3):
+    """(best wall seconds of `repeats` calls after one warm-up call, last result)."""
+    out = fn()
+    best = float("inf")
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        out = fn()
+        best = min(best, time.perf_counter() - t0)
+    return best, out
+
+
+def aux_slice(aux_data, n_aux, frac):
+    """The auxiliary primitives of the shells whose first function lies in the
+    first `frac` of the auxiliary functions (same n_aux: a slice of the output)."""
+    from copy import copy
+
+    import numpy as np
+
+    out = {}
+    for lk, a in aux_data.items():
+        keep = np.asarray(a.i_ao_start) < frac * n_aux
+        if keep.any():
+            b = copy(a)
+            b.A_a = np.ascontiguousarray(a.A_a[keep])
+            b.coefficient = np.ascontiguousarray(np.asarray(a.coefficient)[keep])
+            b.i_ao_start = np.ascontiguousarray(np.asarray(a.i_ao_start)[keep])
+            out[lk] = b
+    return out
+
+
+def run_config0(seed=0):
+    """10-water cluster (30 atoms), O 3s2p1d / H 2s1p, aux s-f, spherical: S, V,
+    (P|Q) and (mu nu|P) through the drop-in C ABI (host arrays in and out, the
+    reference front end's per-class calls), each timed as best of 3 after a
+    warm-up; the reference library (oracle/_ref) on the same inputs with all
+    host threads and with 1 thread ((mu nu|P) at 1 thread on the first eighth
+    of the auxiliary functions); max |GPU - reference| per type."""
+    import importlib
+
+    import numpy as np
+
+    import oracle
+
+    syn = importlib.import_module("electron-integral-playground_b200.synthetic")
+    pu = importlib.import_module("electron-integral-playground_b200.pair_utility")
+    mi = importlib.import_module("electron-integral-playground_b200.molecular_integral")
+    rf = importlib.import_module("electron-integral-playground_b200.roofline")
+    mol = syn.water10_cluster(seed)
+    pd, ad = pu.form_pair_data(mol, 1e-14), pu.form_auxiliary_pair_data(mol)
+    charges = np.asarray(mol.geometry, dtype=np.float64)
+    tot, _ = rf.totals([rf.class_statistics(pd, ad, THRESHOLD)])
+    gpu = {"S": lambda: mi.overlap(pd, mol), "V": lambda: mi.nuclear_attraction(pd, mol, charges),
+           "PQ": lambda: mi.two_center(ad, mol), "3c": lambda: mi.three_center(pd, ad, mol)}
+    out = {"workload": "10 waters in a 9 A cube (30 atoms), orbital O 3s2p1d / H 2s1p contracted, aux s-f, "
+                       f"spherical; n_ao {mol.n_ao}, n_aux {mol.n_aux}",
+           "primitive_pairs": int(sum(p.P_p.shape[0] for p in pd.values())),
+           "aux_primitives": int(sum(a.A_a.shape[0] for a in ad.values())),
+           "primitive_triplets_3c": int(tot["primitive"]), "screened_triplets_3c": int(tot["screened"]),
+           "what": "wall time per integral type through the drop-in entry points (H2D, kernels, D2H, host "
+                   "scatter into the dense reference layout); best of 3 after one warm-up", "types": {}}
+    res = {}
+    for k, f in gpu.items():
+        t, v = best_of(f)
+        res[k] = v
+        out["types"][k] = {"gpu_ms": t * 1e3}
+    ref = oracle.reference()
+    if ref is None:
+        out["reference"] = "reference library not built (make -C oracle ref)"
+        return out
+    nproc = os.cpu_count() or 1
+    refs = {"S": lambda: oracle.drive_overlap(ref, pd, mol),
+            "V": lambda: oracle.drive_nuclear_attraction(ref, pd, mol, charges),
+            "PQ": lambda: oracle.drive_two_center(ref, ad, mol),
+            "3c": lambda: oracle.drive_three_center(ref, pd, ad, mol)}
+    oracle.set_reference_threads(nproc)
+    for k, f in refs.items():
+        t, v = best_of(f, 2)
+        d = out["types"][k]
+        d["reference_ms_all_threads"] = t * 1e3
+        d["max_abs_gpu_vs_reference"] = float(np.max(np.abs(res[k] - v)))
+        d["gpu_speedup_vs_all_threads"] = t * 1e3 / d["gpu_ms"]
+    res = None
+    oracle.set_reference_threads(1)
+    for k in ("S", "V", "PQ"):
+        t, _ = best_of(refs[k], 1)
+        out["types"][k]["reference_ms_1_thread"] = t * 1e3
+    sl = aux_slice(ad, mol.n_aux, 0.125)
+    sl_tot, _ = rf.totals([rf.class_statistics(pd, sl, THRESHOLD)])
+    t, _ = best_of(lambda: oracle.drive_three_center(ref, pd, sl, mol), 1)
+    oracle.set_reference_threads(nproc)
+    t_full = out["types"]["3c"]["reference_ms_all_threads"] * 1e-3
+    out["types"]["3c"].update({
+        "reference_1_thread_slice": {"ms": t * 1e3, "primitive_triplets": int(sl_tot["primitive"]),
+                                     "what": "first eighth of the auxiliary functions, 1 thread"},
+        "reference_1_thread_primitive_triplets_per_s": sl_tot["primitive"] / t,
+        "reference_all_threads_primitive_triplets_per_s": tot["primitive"] / t_full,
+        "gpu_primitive_triplets_per_s": tot["primitive"] / (out["types"]["3c"]["gpu_ms"] * 1e-3),
+        "gpu_screened_triplets_per_s": tot["screened"] / (out["types"]["3c"]["gpu_ms"] * 1e-3)})
+    out["reference"] = {"kind": "reference", "threads_all": nproc, "cpu_model": oracle.cpu_model()}
+    return out
+
+
 def run_reference_arm(args):
     rank, world, _ = rank_info()
     if rank != 0:

@@ -317,7 +317,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sU = reinterpret_cast<double*>(smem_raw);                   // [UB][NU][32], KS > 1
     T* sR = reinterpret_cast<T*>(sU + (C::KS == 1 ? 0 : UB * NU * 32));  // [NRN][32], entries R0..NR-1
-    T* sE = sR + C::NR * 32;                            // [UB][3 NE]
+    T* sE = sR + C::NRN * 32;                           // [UB][3 NE]
     __shared__ int s_item;
 
     const int lane = threadIdx.x & 31;

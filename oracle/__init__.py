@@ -150,4 +150,24 @@ def drive_overlap(lib, pair_data, molecule):
 
 
 def set_reference_threads(n):
+    """OpenMP threads of the reference library's parallel loops in this
+    process (the library is already loaded, so the environment variable alone
+    would not reach it: set the runtime's default thread count as well)."""
     os.environ["OMP_NUM_THREADS"] = str(n)
+    try:
+        ctypes.CDLL("libgomp.so.1").omp_set_num_threads(ctypes.c_int(int(n)))
+        return True
+    except OSError:
+        return False
+
+
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
