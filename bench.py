@@ -11,9 +11,11 @@ buffer.  Metric unit: contracted shell triplets with Schwarz-type bound
   value   device-resident tables, K graph launches timed with CUDA events on
           the library's stream;
   e2e     through the C ABI each step: H2D copy of every input table from the
-          batch's pinned host copy, the graph, and a D2H read of the step's
-          result (one checksum per molecule, accumulated in the kernels'
-          epilogue);
+          batch's pinned host copy and of the 64 molecules' densities, the
+          graph, the density-fitted Coulomb matrix of every molecule (the
+          library's gamma and J kernels over the packed output, Cholesky
+          solves with factors made once per geometry), and a D2H copy of the
+          64 J matrices;
   roofline  the class kernel with the largest device time, run alone,
           algorithmic FLOPs (roofline.py) / its CUDA-event time, against the
           FP64 FMA peak measured on the same GPU by the library's
@@ -21,12 +23,19 @@ buffer.  Metric unit: contracted shell triplets with Schwarz-type bound
   cpu_baseline  the reference library (oracle/_ref, its own C++/OpenMP path)
           on a bounded sample of the same molecules, all host cores.
 
-Also in the line (not part of the timed step): `dropin_fp64`, the plain FP64
-drop-in three_center on the cpu_baseline's sample; `serving`, a Poisson stream
-of 5-200-atom requests (S, V, (P|Q), (mu nu|P)) through the continuous-batching
-server, p50/p99 latency, beside the same requests served alone in FP64;
-`water100_mixed_vs_fp64`, the 100-water cluster's (mu nu|P) in FP64 and mixed
-precision window by window, max abs/rel error per class and triplets/s of both.
+Also in the line (not part of the timed step): `cpu_baseline.gpu_same_sample`,
+the batched GPU path on exactly the CPU sample's molecules; `dropin_fp64`, the
+plain FP64 drop-in three_center on that sample; `serving`, Poisson streams of
+5-200-atom requests (S, V, (P|Q), (mu nu|P)) at several rates through the
+continuous-batching server, p50/p99 latency, beside the same requests served
+alone in FP64; `water100_mixed_vs_fp64`, the 100-water cluster's (mu nu|P) in
+FP64 and mixed precision window by window, max abs/rel error per class and
+triplets/s of both; `water10_per_type`, the 10-water S, V, (P|Q), (mu nu|P)
+through the drop-in beside the reference library at all host threads and 1
+thread; `random_triplets_high_l`, 2000 random shell triplets up to (g g|h) in
+FP64 and mixed precision against the reference library; `mixed_vs_reference`,
+the mixed path's error against the reference library per integral type and
+class.
 
 `--impl reference` times only that reference path (per step: the sample) and
 prints its own line.  Under torchrun each rank runs its own 64 molecules
@@ -189,6 +198,34 @@ def mixed_error(bt, mols, pds, ads, threshold, torch, budget_bytes=30e9):
     return out
 
 
+def same_sample_rate(bt, torch, mols, pds, ads, smp, args):
+    """The batched GPU path (FP64 and mixed) on exactly the cpu_baseline's
+    molecules, CUDA events: screened triplets/s like for like."""
+    idx = smp["molecules"]
+    out = {}
+    for prec in ("fp64", "mixed"):
+        b = bt.ThreeCenterBatch([mols[i] for i in idx], [pds[i] for i in idx], [ads[i] for i in idx],
+                                precision=prec, fp32_threshold=args.fp32_threshold)
+        b.alloc_output()
+        st = torch.cuda.ExternalStream(b.stream)
+        for _ in range(args.warmup):
+            b.run(sync=False)
+        b.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            b.run(sync=False)
+        e1.record(st)
+        b.sync()
+        b.status()
+        ms = e0.elapsed_time(e1) / args.steps
+        out[prec] = {"ms_per_step": ms, "value": smp["triplets"] / (ms * 1e-3)}
+        b.close()
+    torch.cuda.empty_cache()
+    out["ratio_mixed_vs_cpu"] = out["mixed"]["value"] / smp["value"]
+    return out
+
+
 def dropin_sample(mols, pds, ads, stats, sample_idx):
     """The plain FP64 drop-in three_center (reference C ABI, host buffers, dense
     output) on the GPU over the cpu_baseline's sample molecules."""
@@ -209,9 +246,11 @@ def dropin_sample(mols, pds, ads, stats, sample_idx):
 
 
 def run_serving(args, torch, seed):
-    """Open-loop Poisson stream of requests (S, V, (P|Q), (mu nu|P)) of 5-200-atom
-    molecules through the continuous-batching server (mixed precision), and the
-    same requests each served alone in FP64."""
+    """Open-loop Poisson streams of requests (S, V, (P|Q), (mu nu|P)) of 5-200-atom
+    molecules (the first `serve_requests` of the seeded 10k-request stream)
+    through the continuous-batching server (mixed precision) at each rate of
+    `serve_rates` (below, near and above the server's capacity), and the first
+    `serve_alone` requests each served alone in FP64 with nothing else in flight."""
     import importlib
 
     import numpy as np
@@ -220,66 +259,51 @@ def run_serving(args, torch, seed):
     sv = importlib.import_module("electron-integral-playground_b200.serving")
     n = args.serve_requests
     sizes = syn.molecule_sizes(n, 5, 200, seed + 7)
-    rng = np.random.default_rng(seed + 11)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
     # requests carry only the molecule: the server builds its pair tables on
     # the device (and the auxiliary tables) after arrival, inside the latency
     mols = [syn.attach_synthetic_basis(syn.organic_molecule(na, seed * 7919 + i), aux_l_max=4, seed=seed)
             for i, na in enumerate(sizes)]
-    reqs = [sv.Request(i, m, arrival=float(t)) for i, (m, t) in enumerate(zip(mols, arrivals))]
     free, _ = torch.cuda.mem_get_info()
     budget = min(150e9, free - 12e9)
     server = sv.IntegralServer(budget_bytes=budget, precision="mixed", fp32_threshold=args.fp32_threshold)
-    warm = sv.Request(-1, mols[0], arrival=0.0)
-    server.serve([warm], realtime=False)
-    # the host side (threads, builds) makes single runs vary: serve the same
-    # stream several times (fresh requests) and report the median run
-    runs = []
-    for _ in range(max(1, args.serve_repeats)):
+    server.serve([sv.Request(-1, mols[0], arrival=0.0)], realtime=False)  # warm-up
+    rates = [float(r) for r in args.serve_rates.split(",") if r.strip()]
+    per_rate = []
+    pieces = None
+    for k, rate in enumerate(rates):
+        arrivals = np.cumsum(np.random.default_rng(seed + 11 + k).exponential(1.0 / rate, n))
+        reqs = [sv.Request(i, m, arrival=float(t)) for i, (m, t) in enumerate(zip(mols, arrivals))]
         server.launches = 0
-        server.host_s = {k: 0.0 for k in server.host_s}
-        fresh = [sv.Request(r.rid, r.molecule, arrival=r.arrival) for r in reqs]
-        runs.append(server.serve(fresh, realtime=True))
-    st = sorted(runs, key=lambda x: x["throughput_rps"])[len(runs) // 2]
-    pieces = sum(len(server.pieces_of(r)) for r in fresh)  # fresh: the last run's requests, tables built
-    low = None
-    if args.serve_rate_low > 0:
-        # the same molecules arriving below the server's capacity: latency is
-        # then service time rather than queueing
-        t_low = np.cumsum(np.random.default_rng(seed + 13).exponential(1.0 / args.serve_rate_low, n))
-        server.launches = 0
-        sl = server.serve([sv.Request(i, m, arrival=float(t)) for i, (m, t) in enumerate(zip(mols, t_low))],
-                          realtime=True)
-        low = {"rate_rps": args.serve_rate_low, "throughput_rps": sl["throughput_rps"], "wall_s": sl["wall_s"],
-               "latency_p50_ms": sl["latency_p50_s"] * 1e3, "latency_p99_ms": sl["latency_p99_s"] * 1e3,
-               "launches": sl["launches"]}
+        server.host_s = {key: 0.0 for key in server.host_s}
+        st = server.serve(reqs, realtime=True)
+        if pieces is None:
+            pieces = sum(len(server.pieces_of(r)) for r in reqs)
+        per_rate.append({"rate_rps": rate, "requests": n, "throughput_rps": st["throughput_rps"],
+                         "wall_s": st["wall_s"], "latency_p50_ms": st["latency_p50_s"] * 1e3,
+                         "latency_p99_ms": st["latency_p99_s"] * 1e3, "launches": st["launches"],
+                         "host_s": st["host_s"]})
     del server
     torch.cuda.empty_cache()
     alone = []
     # the same work per request as served (S included), nothing else in flight
     solo = sv.IntegralServer(budget_bytes=budget, precision="fp64", max_inflight=1)
-    for r in reqs[:args.serve_alone]:
-        one = sv.Request(r.rid, r.molecule, arrival=0.0)
-        alone.append(solo.serve([one], realtime=False)["latency_p50_s"])
+    for i, m in enumerate(mols[:args.serve_alone]):
+        alone.append(solo.serve([sv.Request(i, m, arrival=0.0)], realtime=False)["latency_p50_s"])
     del solo
     torch.cuda.empty_cache()
     lat_alone = np.array(alone)
-    frac = len(alone) / n
     return {
-        "requests": n, "rate_rps": args.serve_rate, "atoms": [int(x) for x in sizes],
-        "budget_gb": budget / 1e9, "precision": "mixed", "launches": st["launches"], "pieces": pieces,
-        "throughput_rps": st["throughput_rps"], "wall_s": st["wall_s"], "host_s": st["host_s"],
-        "runs_throughput_rps": [r["throughput_rps"] for r in runs], "runs_note": "median run reported",
-        "latency_p50_ms": st["latency_p50_s"] * 1e3, "latency_p99_ms": st["latency_p99_s"] * 1e3,
-        "same_requests_below_capacity": low,
+        "requests": n, "atoms": [int(x) for x in sizes], "budget_gb": budget / 1e9, "precision": "mixed",
+        "pieces": pieces, "rates": per_rate,
         "alone_fp64": {"requests": len(alone), "sum_s": float(lat_alone.sum()),
                        "throughput_rps": len(alone) / float(lat_alone.sum()),
                        "latency_p50_ms": float(np.percentile(lat_alone, 50)) * 1e3,
                        "latency_p99_ms": float(np.percentile(lat_alone, 99)) * 1e3,
-                       "note": "each request served alone (nothing else in flight), FP64, same work (S, V, (P|Q), (mu nu|P))"
-                               + ("" if frac == 1 else f", first {len(alone)} requests")},
-        "sample": f"{n} of the 10k-request stream (Poisson {args.serve_rate} req/s, 5-200 atoms log-uniform); "
-                  "requests carry molecules, pair tables are built on the device after arrival",
+                       "note": "each request served alone (nothing else in flight), FP64, same work "
+                               f"(S, V, (P|Q), (mu nu|P)); first {len(alone)} requests"},
+        "sample": f"the first {n} requests of the seeded 10k-request stream (5-200 atoms log-uniform), "
+                  f"Poisson arrivals at each rate; requests carry molecules, pair tables are built on the "
+                  f"device after arrival",
     }
 
 
@@ -472,6 +496,165 @@ def run_config0(seed=0):
     return out
 
 
+def run_config3(torch, bt, fp64_peak, steps=5, seed=0):
+    """2000 random shell triplets (orbital l <= 4, aux l <= 5, 1-8 primitives,
+    exponents log-uniform in [0.05, 1e4], centres in a 6 A cube), each its own
+    molecule slot of one batch: FP64 and mixed precision, one CUDA-graph launch
+    per step timed with CUDA events; triplets/s, integrals/s, the step's
+    algorithmic FP64 rate; both against the reference library per triplet
+    (max |error| per class, scaled by max(1, max|reference|)) and the reference
+    library's own time for the 2000 calls (all host threads and 1 thread)."""
+    import importlib
+
+    import numpy as np
+
+    import oracle
+
+    syn = importlib.import_module("electron-integral-playground_b200.synthetic")
+    rf = importlib.import_module("electron-integral-playground_b200.roofline")
+    lm = importlib.import_module("electron-integral-playground_b200._lib")
+    trip = syn.random_shell_triplets(seed, 2000)
+    mols = [t[4] for t in trip]
+    pds = [{t[0]: t[1]} for t in trip]
+    ads = [{t[2]: t[3]} for t in trip]
+    flops = sum(t[1].P_p.shape[0] * t[3].A_a.shape[0] * rf.flops_per_primitive_triplet(t[0][0], t[0][1], t[2])
+                for t in trip)
+    out = {"workload": "2000 random shell triplets: orbital l <= 4 (g), auxiliary l <= 5 (h), 1-8 primitives, "
+                       "exponents log-uniform in [0.05, 1e4], centres in a 6 A cube; one molecule slot each",
+           "triplets": 2000, "algorithmic_flops_per_step": flops}
+    dense = {}
+    for prec in ("fp64", "mixed"):
+        b = bt.ThreeCenterBatch(mols, pds, ads, precision=prec)
+        b.alloc_output()
+        st = torch.cuda.ExternalStream(b.stream)
+        for _ in range(3):
+            b.run(sync=False)
+        b.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            b.run(sync=False)
+        e1.record(st)
+        b.sync()
+        b.status()
+        ms = e0.elapsed_time(e1) / steps
+        out[prec] = {"ms_per_step": ms, "triplets_per_s": 2000 / (ms * 1e-3),
+                     "integrals_per_s": b.output_elems / (ms * 1e-3), "launches_per_step": b.launches_per_run}
+        if prec == "fp64":
+            out[prec]["achieved_tflops"] = flops / (ms * 1e-3) / 1e12
+            out[prec]["frac_of_fp64_peak"] = flops / (ms * 1e-3) / 1e12 / fp64_peak
+        buf = np.empty(b.output_elems)
+        b._check(b.L.eip_batch_copy_output(b.h, 0, b.output_elems, lm.dp(buf)), "copy")
+        dense[prec] = (b, buf)
+    ref = oracle.reference()
+    f64, mix = dense["fp64"][0], dense["mixed"][0]
+    out["mixed_vs_fp64_max_abs"] = float(np.max(np.abs(dense["fp64"][1] - dense["mixed"][1])))
+    if ref is not None:
+        nproc = os.cpu_count() or 1
+        per_class = {}
+        t_all, above = 0.0, []
+        oracle.set_reference_threads(nproc)
+        for m, (lij, pair, lk, aux, mol) in enumerate(trip):
+            t0 = time.perf_counter()
+            want = oracle.drive_three_center(ref, {lij: pair}, {lk: aux}, mol)
+            t_all += time.perf_counter() - t0
+            scale = max(1.0, float(np.max(np.abs(want))))
+            e64 = float(np.max(np.abs(f64.dense(m) - want))) / scale
+            emx = float(np.max(np.abs(mix.dense(m) - want))) / scale
+            key = f"{lij[0]}{lij[1]}|{lk}"
+            if e64 > 1e-12:
+                above.append(m)
+            c = per_class.setdefault(key, [0, 0.0, 0.0])
+            c[0] += 1
+            c[1] = max(c[1], e64)
+            c[2] = max(c[2], emx)
+        oracle.set_reference_threads(1)
+        t0 = time.perf_counter()
+        for (lij, pair, lk, aux, mol) in trip[:200]:
+            oracle.drive_three_center(ref, {lij: pair}, {lk: aux}, mol)
+        t_one = (time.perf_counter() - t0) * 10
+        oracle.set_reference_threads(nproc)
+        out["vs_reference"] = {
+            "what": "max over the class's triplets of max|GPU - reference| / max(1, max|reference|)",
+            "fp64_worst": max(v[1] for v in per_class.values()), "mixed_worst": max(v[2] for v in per_class.values()),
+            "fp64_triplets_above_1e-12": above,
+            "by_class": {k: {"triplets": v[0], "fp64": v[1], "mixed": v[2]} for k, v in sorted(per_class.items())}}
+        out["reference"] = {"seconds_all_threads": t_all, "triplets_per_s_all_threads": 2000 / t_all,
+                            "seconds_1_thread": t_one, "triplets_per_s_1_thread": 2000 / t_one,
+                            "threads_all": nproc, "cpu_model": oracle.cpu_model(),
+                            "note": "1-thread time measured on the first 200 triplets, scaled to 2000"}
+    f64.close()
+    mix.close()
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_mixed_vs_reference(bt, mols, pds, ads, threshold, max_dense=4e7, n_take=4):
+    """The mixed-precision served/batched path against the reference library
+    (oracle/_ref, FP64) per integral type and, for (mu nu|P), per class, on the
+    first n_take molecules of the batch whose dense (mu nu|P) stays below
+    max_dense doubles: max abs and max rel (|value| > 1e-6) error."""
+    import importlib
+
+    import numpy as np
+
+    import oracle
+
+    mi = importlib.import_module("electron-integral-playground_b200.molecular_integral")
+    ref = oracle.reference()
+    if ref is None:
+        return None
+    take = [i for i, m in enumerate(mols) if m.n_aux * m.n_ao * m.n_ao <= max_dense][:n_take]
+
+    def err(a, b):
+        d = np.abs(a - b)
+        big = np.abs(b) > 1e-6
+        return [float(d.max()) if d.size else 0.0, float((d[big] / np.abs(b[big])).max()) if big.any() else 0.0]
+
+    def merge(acc, key, e):
+        cur = acc.setdefault(key, [0.0, 0.0])
+        acc[key] = [max(cur[0], e[0]), max(cur[1], e[1])]
+
+    sub = [mols[i] for i in take], [pds[i] for i in take], [ads[i] for i in take]
+    charges = [np.asarray(mols[i].geometry, dtype=np.float64) for i in take]
+    b = bt.ThreeCenterBatch(*sub, precision="mixed", fp32_threshold=threshold, charges_list=charges)
+    b.alloc_output()
+    b.run()
+    b.status()
+    bm = bt.ThreeCenterBatch(sub[0], [bt.metric_pair_tables(a) for a in sub[2]], sub[2], precision="mixed",
+                             fp32_threshold=threshold)
+    bm.alloc_output()
+    bm.run()
+    bm.status()
+    types, classes = {}, {}
+    for k, i in enumerate(take):
+        mol, pd, ad = mols[i], pds[i], ads[i]
+        want = oracle.drive_three_center(ref, pd, ad, mol)
+        got = b.dense(k)
+        merge(types, "3c", err(got, want))
+        # per class: the elements of aux shells of l_k and orbital shells of l_i, l_j
+        ao_of = {}
+        for (li, lj), p in pd.items():
+            for l, st in ((li, p.i_ao_start), (lj, p.j_ao_start)):
+                ao_of.setdefault(l, set()).update(int(s) + c for s in np.unique(st) for c in range(2 * l + 1))
+        for lk, a in ad.items():
+            rows = np.array(sorted({int(s) + c for s in np.unique(a.i_ao_start) for c in range(2 * lk + 1)}))
+            for (li, lj) in pd:
+                A, B = np.array(sorted(ao_of[li])), np.array(sorted(ao_of[lj]))
+                sl = np.ix_(rows, A, B)
+                merge(classes, f"{li}{lj}|{lk}", err(got[sl], want[sl]))
+        merge(types, "V", err(b.dense_V(k), oracle.drive_nuclear_attraction(ref, pd, mol, charges[k])))
+        merge(types, "PQ", err(bm.dense_metric(k), oracle.drive_two_center(ref, ad, mol)))
+        merge(types, "S", err(mi.overlap(pd, mol), oracle.drive_overlap(ref, pd, mol)))
+    b.close()
+    bm.close()
+    return {"molecules": take, "atoms": [len(mols[i].elements) for i in take], "fp32_threshold": threshold,
+            "what": "max abs / max rel (|reference| > 1e-6) of the mixed-precision path vs the reference library; "
+                    "V and (P|Q) run FP64 inside the mixed path, S is the FP64 drop-in",
+            "by_type": {k: {"max_abs": v[0], "max_rel": v[1]} for k, v in types.items()},
+            "by_class_3c": {k: {"max_abs": v[0], "max_rel": v[1]} for k, v in sorted(classes.items())}}
+
+
 def run_reference_arm(args):
     rank, world, _ = rank_info()
     if rank != 0:
@@ -511,12 +694,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fp32-threshold", type=float, default=1e-3,
                     help="mixed precision: FP32 for shell pairs with bound below this")
-    ap.add_argument("--serve-requests", type=int, default=24, help="serving sample: requests (0 = skip)")
-    ap.add_argument("--serve-rate", type=float, default=20.0, help="serving sample: Poisson arrival rate, req/s")
-    ap.add_argument("--serve-alone", type=int, default=24, help="requests also timed alone in FP64")
-    ap.add_argument("--serve-repeats", type=int, default=3, help="serving runs of the stream (median reported)")
-    ap.add_argument("--serve-rate-low", type=float, default=2.0,
-                    help="the same requests again at this Poisson rate (below capacity); 0 = skip")
+    ap.add_argument("--serve-requests", type=int, default=120, help="serving sample: requests (0 = skip)")
+    ap.add_argument("--serve-rates", default="2,4,20",
+                    help="serving sample: Poisson arrival rates, req/s (comma-separated)")
+    ap.add_argument("--serve-alone", type=int, default=40, help="requests also timed alone in FP64")
+    ap.add_argument("--no-config0", action="store_true", help="skip the 10-water per-type timings")
+    ap.add_argument("--no-config3", action="store_true", help="skip the 2000 high-l random triplets")
+    ap.add_argument("--no-mixed-reference", action="store_true",
+                    help="skip the mixed-precision error against the reference library")
     ap.add_argument("--no-config2", action="store_true",
                     help="skip the 100-water mixed-vs-FP64 per-class measurement")
     ap.add_argument("--tune", action="store_true",
@@ -573,10 +758,28 @@ def main():
     mixed.bind_output(out_ptr)  # same layout; the two paths run one after the other
     table_bytes = {"fp64": batch.table_bytes, "mixed": mixed.table_bytes}
     out_bytes = batch.output_bytes
+    # End-to-end product: the density-fitted Coulomb matrix of every molecule
+    # for a density given per step.  The (P|Q) Cholesky factors depend only on
+    # the geometry and auxiliary basis (like the pair tables) and are made once
+    # here; per step: tables and densities in, (mu nu|P), gamma, solve, J, J out.
+    dfm = importlib.import_module("electron-integral-playground_b200.density_fitting")
+    factors = []
+    for m, ad in zip(mols, ads):
+        M = dfm.metric_matrix(torch, m, ad)
+        factors.append(torch.linalg.cholesky(M))
+        del M
+    rng_d = np.random.default_rng(args.seed + 17)
+    dens = []
+    for m in mols:
+        C = rng_d.standard_normal((m.n_ao, max(1, m.n_ao // 8)))
+        dens.append((C @ C.T / m.n_ao).ravel())
+    D_pin = torch.from_numpy(np.concatenate(dens)).pin_memory()
+    D_dev = torch.empty_like(D_pin, device="cuda")
 
     def measure(b, clocks_path):
         """K graph launches timed with CUDA events on b's stream (value), then K
-        end-to-end steps (H2D tables + graph + D2H checksums)."""
+        end-to-end steps (H2D tables and densities, graph, density-fitted J of
+        every molecule, D2H of J)."""
         stream = torch.cuda.ExternalStream(b.stream)
         for _ in range(args.warmup):
             b.run(sync=False)
@@ -595,12 +798,18 @@ def main():
         if world > 1:
             total = reduce_over_ranks([total], torch.distributed.ReduceOp.MAX, "cuda")[0]
         b.status()
-        h_ck = np.empty(len(mols))
+        bc = dfm.BatchCoulomb(torch, b, factors)
+        J_pin = torch.empty(bc.n_ao2, dtype=torch.float64).pin_memory()
 
         def e2e_step():
             b.upload()
-            b.run(checksum=True, sync=False)
-            b._check(b.L.eip_batch_checksums(b.h, lm.dp(h_ck)), "checksums")
+            with torch.cuda.stream(stream):
+                D_dev.copy_(D_pin, non_blocking=True)
+            b.run(sync=False)
+            bc.run(D_dev)
+            with torch.cuda.stream(stream):
+                J_pin.copy_(bc.J[:bc.n_ao2], non_blocking=True)
+            stream.synchronize()
 
         for _ in range(2):
             e2e_step()
@@ -616,8 +825,19 @@ def main():
         e2e = e0.elapsed_time(e1) / args.steps
         if world > 1:
             e2e = reduce_over_ranks([e2e], torch.distributed.ReduceOp.MAX, "cuda")[0]
+        # the consumer kernels alone (gamma, J) on the resident output, CUDA events
+        g0, g1, g2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        g0.record(stream)
+        b.df_gamma(D_dev.data_ptr(), bc.gamma.data_ptr())
+        g1.record(stream)
+        b.df_coulomb(bc.c.data_ptr(), bc.J.data_ptr())
+        g2.record(stream)
+        torch.cuda.synchronize()
+        j_check = float(J_pin.abs().sum())
         return {"ms": total / args.steps, "per_step": per_step, "e2e_ms": e2e, "e2e_wall_ms": wall,
-                "clocks": cs.summary(local), "launches": b.launches_per_run * args.steps}
+                "clocks": cs.summary(local), "launches": b.launches_per_run * args.steps,
+                "df_gamma_ms": g0.elapsed_time(g1), "df_coulomb_ms": g1.elapsed_time(g2), "j_abs_sum": j_check,
+                "h2d": b.table_bytes + 8 * D_pin.numel(), "d2h": 8 * bc.n_ao2}
 
     import tempfile
 
@@ -625,6 +845,9 @@ def main():
     cpath = lambda tag: os.path.join(cdir, f"eip_clocks_{tag}_rank{rank}_{os.getpid()}.csv")
     m64 = measure(batch, cpath("fp64"))
     mmix = measure(mixed, cpath("mixed"))
+    factors.clear()  # the (P|Q) factors (about 14 GB) are not needed below
+    del D_dev
+    torch.cuda.empty_cache()
     split64 = split32 = 0
     for (li, lj, lk) in per_class:
         sp = mixed.precision_split(li, lj, lk)
@@ -718,12 +941,25 @@ def main():
     cpu = None
     dropin = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        oracle.set_reference_threads(os.cpu_count() or 1)
         smp = reference_sample(mols, pds, ads, stats, args.ref_budget)
         if smp is not None:
             cpu = {"value": smp["value"], "unit": UNIT, "cores": smp["cores"], "kind": "reference",
+                   "cpu_model": oracle.cpu_model(),
                    "sample": f"molecules {smp['molecules']} of the batch (dense output <= 2e8 doubles each), "
-                             f"{smp['triplets']} screened triplets, {smp['seconds']:.1f} s"}
+                             f"{smp['triplets']} screened triplets, {smp['seconds']:.1f} s, all host threads",
+                   "gpu_same_sample": same_sample_rate(bt, torch, mols, pds, ads, smp, args)}
             dropin = dropin_sample(mols, pds, ads, stats, smp["molecules"])
+    config0 = config3 = mixed_ref = None
+    if rank == 0 and world == 1:
+        if not args.no_config0:
+            config0 = run_config0(args.seed)
+        if not args.no_config3:
+            config3 = run_config3(torch, bt, fp64_peak, seed=args.seed)
+        if not args.no_mixed_reference:
+            mixed_ref = run_mixed_vs_reference(bt, mols, pds, ads, args.fp32_threshold)
     serving = run_serving(args, torch, args.seed) if args.serve_requests > 0 and rank == 0 else None
     config2 = run_config2(torch, bt, args.fp32_threshold, args.seed) if not args.no_config2 and rank == 0 else None
     if rank == 0:
@@ -742,6 +978,12 @@ def main():
                        "packed_output_bytes": out_bytes, "input_table_bytes": table_bytes,
                        "l2": "inputs + packed output per step exceed the 126 MB L2 (no flush needed)",
                        "parallelism": f"{world} independent shard(s)"},
+            "serving_summary": None if serving is None else {
+                "requests_per_rate": serving["requests"],
+                "rates": [{k: r[k] for k in ("rate_rps", "throughput_rps", "latency_p50_ms", "latency_p99_ms")}
+                          for r in serving["rates"]],
+                "alone_fp64_rps": serving["alone_fp64"]["throughput_rps"],
+                "alone_fp64_p50_ms": serving["alone_fp64"]["latency_p50_ms"]},
             "precision": {"fp64_value": screened / (m64["ms"] * 1e-3), "fp64_ms_per_step": m64["ms"],
                           "mixed_value": screened / (mmix["ms"] * 1e-3), "mixed_ms_per_step": mmix["ms"],
                           "fp32_threshold": args.fp32_threshold,
@@ -751,13 +993,20 @@ def main():
             "integrals_per_s": {"value": out_elems_total / (head["ms"] * 1e-3),
                                 "what": "spherical (mu nu|P) values written per second (packed, i<=j shell pairs)"},
             "e2e": {"value": screened / (head["e2e_ms"] * 1e-3), "unit": UNIT,
-                    "h2d_bytes_per_step": table_bytes["mixed" if mixed_ok else "fp64"],
-                    "d2h_bytes_per_step": 8 * len(mols),
-                    "wall_ms_per_step": head["e2e_wall_ms"],
+                    "h2d_bytes_per_step": head["h2d"], "d2h_bytes_per_step": head["d2h"],
+                    "ms_per_step": head["e2e_ms"], "wall_ms_per_step": head["e2e_wall_ms"],
                     "fp64_value": screened / (m64["e2e_ms"] * 1e-3),
-                    "result": "per-molecule checksum of the packed (mu nu|P) (computed in the kernels' epilogue)"},
+                    "result": "density-fitted Coulomb matrix J of every molecule (gamma = (mu nu|P) D, "
+                              "c = (P|Q)^-1 gamma, J = (mu nu|P) c) copied to pinned host memory each step; "
+                              "inputs per step: every pair/auxiliary table and the 64 densities, from pinned "
+                              "host memory; (P|Q) Cholesky factors made once per geometry before timing",
+                    "df_kernels_ms": {"gamma": head["df_gamma_ms"], "coulomb": head["df_coulomb_ms"],
+                                      "bytes_read_each": out_bytes,
+                                      "gamma_gbs": out_bytes / (head["df_gamma_ms"] * 1e-3) / 1e9,
+                                      "coulomb_gbs": out_bytes / (head["df_coulomb_ms"] * 1e-3) / 1e9}},
             "roofline": roof, "cpu_baseline": cpu, "dropin_fp64": dropin, "serving": serving,
-            "water100_mixed_vs_fp64": config2,
+            "water100_mixed_vs_fp64": config2, "water10_per_type": config0, "random_triplets_high_l": config3,
+            "mixed_vs_reference": mixed_ref,
             "gpu_launches": head["launches"], "clocks": head["clocks"], "clocks_fp64": m64["clocks"],
             "latency_ms": {"p50": statistics.median(per), "p99": sorted(per)[min(len(per) - 1, int(0.99 * len(per)))],
                            "what": "per-step (whole batch) device time; request latency is under serving"},

@@ -59,12 +59,12 @@ int fast3c_set_variant_fp32(int li, int lj, int lk, int v) {
 }
 
 // Doubles of one primitive pair's E record (e_record<li, lj>() in k3c_fast.cuh):
-// E^{0 b}_t, b <= l_i + l_j (l_i > 0 only), then E^{i j}_t, for x, y and z.
+// E^{0 b}_t, b <= l_i + l_j (l_i > 0, l_j >= 2 only), then E^{i j}_t, for x, y and z.
 size_t e_table_doubles(int li, int lj) {
     size_t n = 0;
     for (int i = 0; i <= li; i++)
         for (int j = 0; j <= lj; j++) n += i + j + 1;
-    const size_t h = li > 0 ? (size_t)(li + lj + 1) * (li + lj + 2) / 2 : 0;
+    const size_t h = li > 0 && lj >= 2 ? (size_t)(li + lj + 1) * (li + lj + 2) / 2 : 0;
     return 3 * (n + h);
 }
 

@@ -21,7 +21,7 @@
 //   * E tables of each primitive pair are precomputed once into the
 //     device-resident pair table (e_table_kernel) and staged per pair into
 //     shared memory;
-//   * FP64 kernels of pair classes with l_i > 0 accumulate the (0, b)
+//   * FP64 kernels of pair classes with l_i > 0, l_j >= 2 accumulate the (0, b)
 //     functions of the pair (l_j <= |b| <= l_i + l_j, Hermite coefficients
 //     E^{0 b}_t around P of a Gaussian on centre B) and move l_i onto centre A
 //     once per contracted block, in the epilogue, by the transfer
@@ -59,17 +59,19 @@ constexpr int kVariants = 6;
 __host__ __device__ constexpr int variant_acc(int v) { return v == 2 || v == 4 ? 24 : (v == 3 ? 96 : 48); }
 __host__ __device__ constexpr int variant_warps(int v) { return v == 1 || v == 3 ? 8 : (v >= 4 ? 24 : 16); }
 
-// E table record of one primitive pair (e_table_kernel): for l_i > 0 first
+// E table record of one primitive pair (e_table_kernel): for l_i > 0, l_j >= 2 first
 // E^{0 b}_t, b <= l_i + l_j, for x, y, z (the transfer-after-contraction
 // kernels), then E^{i j}_t for x, y, z (the direct kernels).
 template <int LI, int LJ>
-__host__ __device__ constexpr int e_hrr_size() { return LI > 0 ? (LI + LJ + 1) * (LI + LJ + 2) / 2 : 0; }
+__host__ __device__ constexpr int e_hrr_size() { return LI > 0 && LJ >= 2 ? (LI + LJ + 1) * (LI + LJ + 2) / 2 : 0; }
 template <int LI, int LJ>
 __host__ __device__ constexpr int e_record() { return 3 * (e_hrr_size<LI, LJ>() + e_size<LI, LJ>()); }
 
-// FP64 kernels of pair classes with l_i > 0 transfer after the contraction.
-template <int LI, typename T>
-constexpr bool use_hrr() { return LI > 0 && std::is_same<T, double>::value; }
+// FP64 kernels of the pair classes with l_i > 0 and l_j >= 2 transfer after
+// the contraction (for p-p the saving, 27 against 33 E-term products, does not
+// pay for the longer epilogue).
+template <int LI, int LJ, typename T>
+constexpr bool use_hrr() { return LI > 0 && LJ >= 2 && std::is_same<T, double>::value; }
 
 template <int LI, int LJ, int LK, int V = 0, bool HRR = false>
 struct Fast3c {
@@ -300,11 +302,11 @@ __device__ __forceinline__ void unit_prefactor(double p, double q, double c, dou
 // zeta = p (omega > 0: p w^2 / (p + w^2)), prefactor c_ab 2 pi / p
 // (omega > 0: c_ab 2 pi w / (p sqrt(p + w^2))), l_k = 0.
 template <int LI, int LJ, int LK, int V, typename T, bool POINT = false>
-__global__ void __launch_bounds__(Fast3c<LI, LJ, LK, V, use_hrr<LI, T>()>::THREADS,
-                                  Fast3c<LI, LJ, LK, V, use_hrr<LI, T>()>::MIN_CTAS)
+__global__ void __launch_bounds__(Fast3c<LI, LJ, LK, V, use_hrr<LI, LJ, T>()>::THREADS,
+                                  Fast3c<LI, LJ, LK, V, use_hrr<LI, LJ, T>()>::MIN_CTAS)
 k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, BatchMap map, double omega,
          double* __restrict__ out, int* __restrict__ work_counter, int total_items) {
-    constexpr bool HRR = use_hrr<LI, T>();
+    constexpr bool HRR = use_hrr<LI, LJ, T>();
     using C = Fast3c<LI, LJ, LK, V, HRR>;
     static_assert(POINT || ket_top_level_only<LK>(), "spherical ket with lower Hermite levels");
     constexpr int L = C::L;
@@ -799,7 +801,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
 template <int LI, int LJ, int LK, int V, typename T, bool POINT = false>
 static int launch_one(const double* boys_table, const BraTable& bra, const KetTable& ket, const BatchMap& map,
                       int total_items, double omega, double* out, int* counter, cudaStream_t s) {
-    using C = Fast3c<LI, LJ, LK, V, use_hrr<LI, T>()>;
+    using C = Fast3c<LI, LJ, LK, V, use_hrr<LI, LJ, T>()>;
     if (total_items <= 0) return 0;
     constexpr size_t smem = C::template smem_bytes<T>();
     static std::atomic<int> max_blocks[kMaxDevices];

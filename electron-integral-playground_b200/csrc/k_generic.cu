@@ -9,20 +9,19 @@
 // one contracted block (shell pair, auxiliary shell or point charge, chunk of
 // ket components), computed as
 //   (mu nu|P) = sum_{prim pairs} sum_{aux prims} pref
-//               sum_{tuv} E^{0 b}_{tuv} sum_s (-1)^{|s|} E^{k}_s R_{t+s_x,u+s_y,v+s_z}
-// for the (0, b) functions of the pair (all b with l_j <= |b| <= l_i + l_j, a
-// Gaussian on centre B of exponent p = a + b), followed once per block by the
-// horizontal transfer (a+1_d, b) = (a, b+1_d) - AB_d (a, b) that moves l_i
-// onto centre A.  AB is the same for every primitive pair of a shell pair, so
-// the transfer commutes with the contraction over primitives (this library's
-// arrangement; the reference transfers E coefficients per primitive pair,
-// c_library/mcmurchie_davidson_E_term.hpp:166-199).  Per block of kGenUB
-// units (primitive pair x auxiliary primitive) the CTA first evaluates, one
-// thread per unit, the prefactor, Boys function, scaled R^{(m)}_000 and
-// coordinate powers, and per unit and axis the E^{0 b}_t table; then, unit by
+//               sum_{tuv} E^{ij}_{tuv} sum_s (-1)^{|s|} E^{k}_s R_{t+s_x,u+s_y,v+s_z}
+// with the two-centre coefficients E^{ij}_t built per primitive pair in FP64
+// (vertical recursion on centre A, then the transfer to centre B,
+// c_library/mcmurchie_davidson_E_term.hpp:22-45, 166-199).  Per block of
+// kGenUB units (primitive pair x auxiliary primitive) the CTA first evaluates,
+// one thread per unit, the prefactor, Boys function, scaled R^{(m)}_000 and
+// coordinate powers, and per unit and axis the E^{ij}_t table; then, unit by
 // unit, all threads split (1) the Hermite tetrahedron R_{tuv} (closed form),
 // (2) the ket contraction X[h][k], (3) the bra contraction into accumulators
-// held in registers (kGenAcc per thread).
+// held in registers (kGenAcc per thread).  (Transferring after the
+// contraction instead, as the fast FP64 kernels do for l <= 2, loses up to
+// 1e-9 to cancellation for g-g pairs with distant centres and extreme
+// exponents, so the high-l classes transfer per primitive pair.)
 //
 // Spherical kets use only the top Hermite level |s| = l_k: a real solid
 // harmonic is a harmonic polynomial, so its Gaussian's Hermite expansion has
@@ -95,23 +94,23 @@ constexpr size_t kGenMaxSmem = 200 * 1024;
 struct GenShape {
     int li, lj, lk, lij, L;
     int point, spherical;
-    int nbase;      // (0, b) functions, l_j <= |b| <= l_i + l_j
+    int nij;        // Cartesian (i, j) pairs of the bra
     int nhb;        // bra Hermite entries, t + u + v <= l_i + l_j
     int n_io, n_jo, n_ko;
     int nkc;        // Cartesian components of l_k
     int ko_chunk, n_chunks;
-    int nea;        // E^{0 b}_t entries per axis, b <= l_i + l_j
+    int nea;        // E^{ij}_t entries per axis: (l_i+1)(l_j+1)(l_i+l_j+1)
     int rmin;       // lowest Hermite order of R the ket reads
     int nr;         // nherm(L)
     int unit_dbl;   // doubles per unit record
-    int maxlev;     // largest transfer level (doubles, one ket component)
     // shared-memory offsets, in doubles
-    int o_unit, o_hr, o_ket, o_dec, o_work, o_x, o_base, o_lev;
+    int o_unit, o_hr, o_ket, o_dec, o_work, o_x, o_base;
     int smem_dbl;
 };
 
 // Unit record: [0, L] R^{(m)}_000 (-2 zeta)^m; L+1 prefactor; then X, Y, Z
-// powers (L+1 each); then E^{0 b}_t for x, y, z (nea each); then, Cartesian
+// powers (L+1 each); then E^{ij}_t for x, y, z (nea each, index
+// (i (l_j+1) + j)(l_i+l_j+1) + t); then, Cartesian
 // kets only, the signed one-centre coefficients (l_k+1)^2.
 __host__ __device__ inline int unit_pow(const GenShape& g) { return g.L + 2; }
 __host__ __device__ inline int unit_e(const GenShape& g) { return g.L + 2 + 3 * (g.L + 1); }
@@ -121,23 +120,21 @@ static GenShape general_shape(int li, int lj, int lk, bool point, bool spherical
     GenShape g{};
     g.li = li; g.lj = lj; g.lk = point ? 0 : lk; g.lij = li + lj; g.L = g.lij + g.lk;
     g.point = point; g.spherical = spherical;
-    g.nbase = nherm(g.lij) - nherm(lj - 1);
+    g.nij = ncart(li) * ncart(lj);
     g.nhb = nherm(g.lij);
     g.n_io = spherical ? nsph(li) : ncart(li);
     g.n_jo = spherical ? nsph(lj) : ncart(lj);
     g.n_ko = point ? 1 : (spherical ? nsph(g.lk) : ncart(g.lk));
     g.nkc = ncart(g.lk);
-    g.ko_chunk = std::max(1, std::min(g.n_ko, kGenThreads * kGenAcc / g.nbase));
+    g.ko_chunk = std::max(1, std::min(g.n_ko, kGenThreads * kGenAcc / g.nij));
     g.n_chunks = (g.n_ko + g.ko_chunk - 1) / g.ko_chunk;
-    g.nea = (g.lij + 1) * (g.lij + 2) / 2;
+    g.nea = (li + 1) * (lj + 1) * (g.lij + 1);
     g.rmin = (spherical && !point) ? g.lk : 0;
     g.nr = nherm(g.L);
     g.unit_dbl = unit_ek(g) + ((!spherical && !point) ? (g.lk + 1) * (g.lk + 1) : 0);
-    g.maxlev = 0;
-    for (int k = 1; k <= li; k++) g.maxlev = std::max(g.maxlev, ncart(k) * (nherm(g.lij - k) - nherm(lj - 1)));
     // layout: unit block | closed-form coefficients | ket rows | tetrahedron
-    // decode (ints) | work region: [R | X] during the unit loop, [base | two
-    // transfer levels] in the epilogue
+    // decode (ints) | work region: [R | X] during the unit loop, the
+    // accumulated Cartesian block in the epilogue
     int o = 0;
     g.o_unit = o; o += kGenUB * g.unit_dbl;
     g.o_hr = o; o += (kGenMaxL + 1) * (kGenMaxL + 1);
@@ -146,9 +143,8 @@ static GenShape general_shape(int li, int lj, int lk, bool point, bool spherical
     g.o_work = o;
     g.o_x = o + g.nr;
     g.o_base = o;
-    g.o_lev = o + g.nbase * g.ko_chunk;
     const int loop_end = g.o_x + g.nhb * g.ko_chunk;
-    const int epi_end = g.o_lev + 2 * g.maxlev;
+    const int epi_end = g.o_base + g.nij * g.ko_chunk;
     g.smem_dbl = std::max(loop_end, epi_end);
     return g;
 }
@@ -164,7 +160,6 @@ general_kernel(const double* __restrict__ boys_table, GenShape g, BraTable bra, 
     double* sR = gsm + g.o_work;
     double* sX = gsm + g.o_x;
     double* sBase = gsm + g.o_base;
-    double* sLev = gsm + g.o_lev;
     __shared__ int s_item;
     const int tid = threadIdx.x;
     // work_counter[0]: next item; work_counter[1]: status (0 ok, else the first
@@ -193,8 +188,8 @@ general_kernel(const double* __restrict__ boys_table, GenShape g, BraTable bra, 
             cart_decode(N, c, x, y, z);
             sDec[nherm(N - 1) + c] = x | (y << 8) | (z << 16);
         }
-    // accumulator entry e = tid + kGenThreads * k holds (base function b, ket component)
-    const int n_ent = g.nbase * g.ko_chunk;
+    // accumulator entry e = tid + kGenThreads * k holds (Cartesian pair ij, ket component)
+    const int n_ent = g.nij * g.ko_chunk;
 
     for (int iter = 0;; iter++) {
         __syncthreads();
@@ -321,23 +316,34 @@ general_kernel(const double* __restrict__ boys_table, GenShape g, BraTable bra, 
                         pz *= Z;
                     }
                 } else {
-                    // E^{0,b+1}_t = E^{0,b}_{t-1} / (2p) + PB E^{0,b}_t + (t+1) E^{0,b}_{t+1}, PB = PA + AB
+                    // E^{i+1,0}_t = E^{i,0}_{t-1} / (2p) + PA E^{i,0}_t + (t+1) E^{i,0}_{t+1}
+                    // for i < l_i + l_j, then E^{i,j+1}_t = E^{i+1,j}_t + AB E^{i,j}_t,
+                    // level j kept in W (rows i <= l_i + l_j - j) and rows i <= l_i stored
                     const int d = (w - nb) % 3;
                     const double4 PA = bra.prim_PA[pp];
-                    const double pb_d = d == 0 ? PA.x + AB.x : (d == 1 ? PA.y + AB.y : PA.z + AB.z);
+                    const double pa_d = d == 0 ? PA.x : (d == 1 ? PA.y : PA.z);
+                    const double ab_d = d == 0 ? AB.x : (d == 1 ? AB.y : AB.z);
                     const double inv2p = 0.5 / P.w;
+                    const int N = g.lij, T1 = g.lij + 1;
                     double* E = U + unit_e(g) + d * g.nea;
-                    E[0] = 1.0;
-                    for (int b = 0; b < g.lij; b++) {
-                        const double* Eb = E + b * (b + 1) / 2;
-                        double* En = E + (b + 1) * (b + 2) / 2;
-                        for (int t = 0; t <= b + 1; t++) {
+                    double W[kMaxOrbitalL * 2 + 1][kMaxOrbitalL * 2 + 1];
+                    for (int i = 0; i <= N; i++)
+                        for (int t = 0; t <= N; t++) W[i][t] = 0.0;
+                    W[0][0] = 1.0;
+                    for (int i = 0; i < N; i++)
+                        for (int t = 0; t <= i + 1; t++) {
                             double v = 0.0;
-                            if (t >= 1) v = inv2p * Eb[t - 1];
-                            if (t <= b) v = fma(pb_d, Eb[t], v);
-                            if (t + 1 <= b) v = fma((double)(t + 1), Eb[t + 1], v);
-                            En[t] = v;
+                            if (t >= 1) v = inv2p * W[i][t - 1];
+                            if (t <= i) v = fma(pa_d, W[i][t], v);
+                            if (t + 1 <= i) v = fma((double)(t + 1), W[i][t + 1], v);
+                            W[i + 1][t] = v;
                         }
+                    for (int j = 0; j <= g.lj; j++) {
+                        for (int i = 0; i <= g.li; i++)
+                            for (int t = 0; t <= N; t++) E[(i * (g.lj + 1) + j) * T1 + t] = W[i][t];
+                        if (j == g.lj) break;
+                        for (int i = 0; i + j + 1 <= N; i++)
+                            for (int t = 0; t <= N; t++) W[i][t] = fma(ab_d, W[i][t], W[i + 1][t]);
                     }
                 }
             }
@@ -401,7 +407,7 @@ general_kernel(const double* __restrict__ boys_table, GenShape g, BraTable bra, 
                     sX[e] = x;
                 }
                 __syncthreads();
-                // (3) bra: acc[(b, k)] += pref sum_t Ex sum_u Ey sum_v Ez X[tuv][k]
+                // (3) bra: acc[(ij, k)] += pref sum_t Ex sum_u Ey sum_v Ez X[tuv][k]
                 {
                     const double pref = U[g.L + 1];
                     const double* Ex = U + unit_e(g);
@@ -411,19 +417,22 @@ general_kernel(const double* __restrict__ boys_table, GenShape g, BraTable bra, 
                     for (int k = 0; k < kGenAcc; k++) {
                         const int e = tid + kGenThreads * k;
                         if (e < n_ent) {
-                            const int b = e / g.ko_chunk, kl = e - b * g.ko_chunk;
+                            const int ij = e / g.ko_chunk, kl = e - ij * g.ko_chunk;
                             if (kl < nkoc) {
-                                const int db = sDec[nherm(g.lj - 1) + b];
-                                const int bx = db & 255, by = (db >> 8) & 255, bz = db >> 16;
-                                const double* ex = Ex + bx * (bx + 1) / 2;
-                                const double* ey = Ey + by * (by + 1) / 2;
-                                const double* ez = Ez + bz * (bz + 1) / 2;
+                                const int ci = ij / ncart(g.lj), cj = ij - ci * ncart(g.lj);
+                                const int da = sDec[nherm(g.li - 1) + ci], db = sDec[nherm(g.lj - 1) + cj];
+                                const int ix = da & 255, iy = (da >> 8) & 255, iz = da >> 16;
+                                const int jx = db & 255, jy = (db >> 8) & 255, jz = db >> 16;
+                                const int T1 = g.lij + 1, J1 = g.lj + 1;
+                                const double* ex = Ex + (ix * J1 + jx) * T1;
+                                const double* ey = Ey + (iy * J1 + jy) * T1;
+                                const double* ez = Ez + (iz * J1 + jz) * T1;
                                 double s = 0.0;
-                                for (int t = 0; t <= bx; t++) {
+                                for (int t = 0; t <= ix + jx; t++) {
                                     double su = 0.0;
-                                    for (int u = 0; u <= by; u++) {
+                                    for (int u = 0; u <= iy + jy; u++) {
                                         double sv = 0.0;
-                                        for (int v = 0; v <= bz; v++)
+                                        for (int v = 0; v <= iz + jz; v++)
                                             sv = fma(ez[v], sX[herm_idx(t, u, v) * nkoc + kl], sv);
                                         su = fma(ey[u], sv, su);
                                     }
@@ -437,70 +446,38 @@ general_kernel(const double* __restrict__ boys_table, GenShape g, BraTable bra, 
             }
         }
         __syncthreads();
-        // Epilogue: base integrals to shared memory, transfer l_i onto centre A,
-        // bra (and, Cartesian, ket) output transform, stores.
+        // Epilogue: the Cartesian block to shared memory, bra (and, Cartesian,
+        // ket) output transform, stores.
 #pragma unroll
         for (int k = 0; k < kGenAcc; k++) {
             const int e = tid + kGenThreads * k;
             if (e < n_ent) sBase[e] = acc[k];
         }
         __syncthreads();
-        const double ab[3] = {AB.x, AB.y, AB.z};
         const size_t obase = (size_t)__ldg(map.out_begin + m);
         double wsum = 0.0;  // this thread's stored values (optional per-molecule checksum)
-        for (int kl = 0; kl < nkoc; kl++) {
-            // level k holds (a, b) for |a| = k and b the first nb_k base functions
-            const double* src = sBase + kl;
-            int src_stride = g.ko_chunk;  // level 0: column kl of the base block
-            int nb_prev = g.nbase;
-            for (int k = 1; k <= g.li; k++) {
-                const int nbk = nherm(g.lij - k) - nherm(g.lj - 1);
-                double* dst = sLev + ((k & 1) ? 0 : g.maxlev);
-                for (int e = tid; e < ncart(k) * nbk; e += kGenThreads) {
-                    const int ai = e / nbk, bi = e - ai * nbk;
-                    int ax, ay, az;
-                    cart_decode(k, ai, ax, ay, az);
-                    const int d = ax > 0 ? 0 : (ay > 0 ? 1 : 2);
-                    if (d == 0) ax--;
-                    else if (d == 1) ay--;
-                    else az--;
-                    const int ap = cart_index(ax, ay, az);
-                    const int db = sDec[nherm(g.lj - 1) + bi];
-                    int bx = db & 255, by = (db >> 8) & 255, bz = db >> 16;
-                    if (d == 0) bx++;
-                    else if (d == 1) by++;
-                    else bz++;
-                    const int bn = nherm(bx + by + bz - 1) - nherm(g.lj - 1) + cart_index(bx, by, bz);
-                    dst[e] = src[(ap * nb_prev + bn) * src_stride] - ab[d] * src[(ap * nb_prev + bi) * src_stride];
-                }
-                __syncthreads();
-                src = dst;
-                src_stride = 1;
-                nb_prev = nbk;
-            }
-            // final level: (a, b) with |a| = l_i, |b| = l_j (b index < ncart(l_j))
+        const int nj_c = ncart(g.lj);
+        for (int e = tid; e < nkoc * g.n_io * g.n_jo; e += kGenThreads) {
+            const int kl = e / (g.n_io * g.n_jo), IJ = e - kl * (g.n_io * g.n_jo);
+            const int I = IJ / g.n_jo, J = IJ - I * g.n_jo;
             const int ko = ko0 + kl;
             const double knorm = (g.spherical || g.point) ? 1.0 : c_cart_norm[c_cart_norm_offset[g.lk] + ko];
-            for (int e = tid; e < g.n_io * g.n_jo; e += kGenThreads) {
-                const int I = e / g.n_jo, J = e - I * g.n_jo;
-                double v = 0.0;
-                for (int ca = 0; ca < ncart(g.li); ca++) {
-                    const double wi = g.spherical ? c_sph_coef[c_sph_offset[g.li] + I * ncart(g.li) + ca]
-                                                  : (I == ca ? c_cart_norm[c_cart_norm_offset[g.li] + ca] : 0.0);
-                    if (wi == 0.0) continue;
-                    double vj = 0.0;
-                    for (int cb = 0; cb < ncart(g.lj); cb++) {
-                        const double wj = g.spherical ? c_sph_coef[c_sph_offset[g.lj] + J * ncart(g.lj) + cb]
-                                                      : (J == cb ? c_cart_norm[c_cart_norm_offset[g.lj] + cb] : 0.0);
-                        if (wj != 0.0) vj = fma(wj, src[(ca * nb_prev + cb) * src_stride], vj);
-                    }
-                    v = fma(wi, vj, v);
+            double v = 0.0;
+            for (int ca = 0; ca < ncart(g.li); ca++) {
+                const double wi = g.spherical ? c_sph_coef[c_sph_offset[g.li] + I * ncart(g.li) + ca]
+                                              : (I == ca ? c_cart_norm[c_cart_norm_offset[g.li] + ca] : 0.0);
+                if (wi == 0.0) continue;
+                double vj = 0.0;
+                for (int cb = 0; cb < nj_c; cb++) {
+                    const double wj = g.spherical ? c_sph_coef[c_sph_offset[g.lj] + J * nj_c + cb]
+                                                  : (J == cb ? c_cart_norm[c_cart_norm_offset[g.lj] + cb] : 0.0);
+                    if (wj != 0.0) vj = fma(wj, sBase[(ca * nj_c + cb) * g.ko_chunk + kl], vj);
                 }
-                const size_t row = (((size_t)sp_k * g.n_io + I) * g.n_jo + J) * g.n_ko + ko;
-                out[obase + row * n_aux + a_local] = v * knorm;
-                wsum += v * knorm;
+                v = fma(wi, vj, v);
             }
-            __syncthreads();
+            const size_t row = (((size_t)sp_k * g.n_io + I) * g.n_jo + J) * g.n_ko + ko;
+            out[obase + row * n_aux + a_local] = v * knorm;
+            wsum += v * knorm;
         }
         if (map.checksum && wsum != 0.0) atomicAdd(map.checksum + m, wsum);
     }
@@ -512,7 +489,8 @@ int general_chunks(int li, int lj, int lk, bool point, bool spherical) {
 
 int launch_general(int li, int lj, int lk, bool point, bool spherical, const BraTable& bra, const KetTable& ket,
                    const BatchMap& map, int total_items, double omega, double* out, int* counter, cudaStream_t s) {
-    if (li < 0 || li > lj || lj > kMaxAuxL || lk < 0 || lk > kMaxAuxL || li + lj + (point ? 0 : lk) > kGenMaxL)
+    if (li < 0 || li > lj || lj > kMaxAuxL || li + lj > 2 * kMaxOrbitalL || lk < 0 || lk > kMaxAuxL ||
+        li + lj + (point ? 0 : lk) > kGenMaxL)
         return 1;
     if (total_items <= 0) return 0;
     const GenShape g = general_shape(li, lj, lk, point, spherical);
