@@ -763,10 +763,12 @@ def main():
     # the geometry and auxiliary basis (like the pair tables) and are made once
     # here; per step: tables and densities in, (mu nu|P), gamma, solve, J, J out.
     dfm = importlib.import_module("electron-integral-playground_b200.density_fitting")
-    factors = []
+    factors, shifts = [], []
     for m, ad in zip(mols, ads):
         M = dfm.metric_matrix(torch, m, ad)
-        factors.append(torch.linalg.cholesky(M))
+        Lf, lam = dfm.metric_factor(torch, M)
+        factors.append(Lf)
+        shifts.append(lam / float(M.diagonal().max()))
         del M
     rng_d = np.random.default_rng(args.seed + 17)
     dens = []
@@ -999,7 +1001,9 @@ def main():
                     "result": "density-fitted Coulomb matrix J of every molecule (gamma = (mu nu|P) D, "
                               "c = (P|Q)^-1 gamma, J = (mu nu|P) c) copied to pinned host memory each step; "
                               "inputs per step: every pair/auxiliary table and the 64 densities, from pinned "
-                              "host memory; (P|Q) Cholesky factors made once per geometry before timing",
+                              "host memory; (P|Q) Cholesky factors made once per geometry before timing "
+                              f"({sum(1 for x in shifts if x > 0)} of {len(shifts)} metrics needed a diagonal "
+                              f"shift, largest {max(shifts):.0e} x max diag)",
                     "df_kernels_ms": {"gamma": head["df_gamma_ms"], "coulomb": head["df_coulomb_ms"],
                                       "bytes_read_each": out_bytes,
                                       "gamma_gbs": out_bytes / (head["df_gamma_ms"] * 1e-3) / 1e9,

@@ -103,6 +103,25 @@ def metric_matrix(torch, molecule, aux_data):
     return M
 
 
+def metric_factor(torch, M, max_shift=1e-8):
+    """Lower Cholesky factor of the metric, FP64 (library call).  Even-tempered
+    auxiliary bases on nearby atoms make (P|Q) nearly singular (condition
+    numbers beyond 1e12), so when the plain factorisation fails the diagonal is
+    raised by the smallest shift lambda = 10^k * max(diag M), k = -15..-8, that
+    lets it complete.  Returns (L, lambda)."""
+    Lf, info = torch.linalg.cholesky_ex(M)
+    if int(info) == 0:
+        return Lf, 0.0
+    scale = float(M.diagonal().max())
+    eye = torch.eye(M.shape[0], dtype=M.dtype, device=M.device)
+    for k in range(-15, int(round(__import__("math").log10(max_shift))) + 1):
+        lam = scale * 10.0 ** k
+        Lf, info = torch.linalg.cholesky_ex(M + lam * eye)
+        if int(info) == 0:
+            return Lf, lam
+    raise RuntimeError("metric not factorisable with a diagonal shift up to max_shift * max(diag)")
+
+
 def coulomb_matrix(molecule, pair_data, aux_data, D, precision="fp64", window_bytes=None, metric=None):
     """Density-fitted J for one molecule.  With window_bytes, (mu nu|P) is
     computed in auxiliary windows of at most that many output bytes over one
