@@ -698,6 +698,8 @@ def main():
     ap.add_argument("--serve-rates", default="2,4,20",
                     help="serving sample: Poisson arrival rates, req/s (comma-separated)")
     ap.add_argument("--serve-alone", type=int, default=40, help="requests also timed alone in FP64")
+    ap.add_argument("--no-e2e-df", dest="e2e_df", action="store_false",
+                    help="e2e returns per-molecule checksums instead of the density-fitted J (profiling runs)")
     ap.add_argument("--no-config0", action="store_true", help="skip the 10-water per-type timings")
     ap.add_argument("--no-config3", action="store_true", help="skip the 2000 high-l random triplets")
     ap.add_argument("--no-mixed-reference", action="store_true",
@@ -764,7 +766,7 @@ def main():
     # here; per step: tables and densities in, (mu nu|P), gamma, solve, J, J out.
     dfm = importlib.import_module("electron-integral-playground_b200.density_fitting")
     factors, shifts = [], []
-    for m, ad in zip(mols, ads):
+    for m, ad in (zip(mols, ads) if args.e2e_df else []):
         M = dfm.metric_matrix(torch, m, ad)
         Lf, lam = dfm.metric_factor(torch, M)
         factors.append(Lf)
@@ -800,6 +802,28 @@ def main():
         if world > 1:
             total = reduce_over_ranks([total], torch.distributed.ReduceOp.MAX, "cuda")[0]
         b.status()
+        if not args.e2e_df:
+            # profiling runs: tables in, the graph, per-molecule checksums out
+            h_ck = np.empty(len(mols))
+
+            def e2e_ck():
+                b.upload()
+                b.run(checksum=True, sync=False)
+                b._check(b.L.eip_batch_checksums(b.h, lm.dp(h_ck)), "checksums")
+
+            for _ in range(2):
+                e2e_ck()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                e2e_ck()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            e2e = e0.elapsed_time(e1) / args.steps
+            return {"ms": total / args.steps, "per_step": per_step, "e2e_ms": e2e, "e2e_wall_ms": e2e,
+                    "clocks": cs.summary(local), "launches": b.launches_per_run * args.steps,
+                    "df_gamma_ms": None, "df_coulomb_ms": None, "j_abs_sum": None,
+                    "h2d": b.table_bytes, "d2h": 8 * len(mols)}
         bc = dfm.BatchCoulomb(torch, b, factors)
         J_pin = torch.empty(bc.n_ao2, dtype=torch.float64).pin_memory()
 
@@ -1003,11 +1027,12 @@ def main():
                               "inputs per step: every pair/auxiliary table and the 64 densities, from pinned "
                               "host memory; (P|Q) Cholesky factors made once per geometry before timing "
                               f"({sum(1 for x in shifts if x > 0)} of {len(shifts)} metrics needed a diagonal "
-                              f"shift, largest {max(shifts):.0e} x max diag)",
-                    "df_kernels_ms": {"gamma": head["df_gamma_ms"], "coulomb": head["df_coulomb_ms"],
-                                      "bytes_read_each": out_bytes,
-                                      "gamma_gbs": out_bytes / (head["df_gamma_ms"] * 1e-3) / 1e9,
-                                      "coulomb_gbs": out_bytes / (head["df_coulomb_ms"] * 1e-3) / 1e9}},
+                              f"shift, largest {max(shifts, default=0):.0e} x max diag)"
+                              if args.e2e_df else "per-molecule checksums (--no-e2e-df profiling run)",
+                    "df_kernels_ms": None if head["df_gamma_ms"] is None else {
+                        "gamma": head["df_gamma_ms"], "coulomb": head["df_coulomb_ms"], "bytes_read_each": out_bytes,
+                        "gamma_gbs": out_bytes / (head["df_gamma_ms"] * 1e-3) / 1e9,
+                        "coulomb_gbs": out_bytes / (head["df_coulomb_ms"] * 1e-3) / 1e9}},
             "roofline": roof, "cpu_baseline": cpu, "dropin_fp64": dropin, "serving": serving,
             "water100_mixed_vs_fp64": config2, "water10_per_type": config0, "random_triplets_high_l": config3,
             "mixed_vs_reference": mixed_ref,
