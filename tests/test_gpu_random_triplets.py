@@ -34,13 +34,22 @@ def test_boys_1e6_samples_against_series():
     assert np.max(rel) < 1e-14, float(np.max(rel))
 
 
+# The triplets of the seeded 2000 whose FP64 value cancels: every one of them
+# has an f or g shell on centre B (l_j >= 3) and extreme exponents, and the
+# reference and this repository's independent C oracle already differ on it
+# by 5e-13 to 2.5e-10.  Only these may exceed
+# 1e-12 (each within 4x that distance); any other triplet must meet 1e-12.
+CANCELLING_TRIPLETS = frozenset({160, 276, 372, 404, 422, 546, 626, 694, 717, 949, 1096, 1117, 1192, 1287, 1377,
+                                 1431, 1526, 1735, 1868, 1880})
+
+
 def test_2000_triplets_fp64_against_reference(triplets):
     """|GPU - reference| <= 1e-12 max(1, max|reference|) for at least 98% of the
     triplets; the rest are high-L triplets with extreme exponents whose FP64
     values cancel: two independent FP64 implementations (the reference and
     this repository's C oracle) already differ on them by up to ~2.5e-10.
-    There the GPU must be within max(1e-11, 4x the oracle-to-reference
-    distance)."""
+    Those triplets are named (CANCELLING_TRIPLETS); there the GPU must be
+    within max(1e-11, 4x the oracle-to-reference distance)."""
     ref = oracle.reference()
     if ref is None:
         pytest.skip("reference library not built")
@@ -58,8 +67,8 @@ def test_2000_triplets_fp64_against_reference(triplets):
     print(f"2000 triplets: max |GPU - reference| / max(1, |reference|) = {worst:.3e}; "
           f"{len(enveloped)} above 1e-12 (triplet, class, GPU error, oracle-reference distance): {enveloped}")
     for n, lij, lk, err, env in enveloped:
+        assert n in CANCELLING_TRIPLETS, (n, lij, lk, err, env)
         assert err <= max(1e-11, 4 * env), (n, lij, lk, err, env)
-    assert len(enveloped) <= 40
 
 
 def test_2000_triplets_mixed_against_fp64(triplets):
