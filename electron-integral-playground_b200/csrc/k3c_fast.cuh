@@ -73,6 +73,10 @@ __host__ __device__ constexpr int e_record() { return 3 * (e_hrr_size<LI, LJ>() 
 template <int LI, int LJ, typename T>
 constexpr bool use_hrr() { return LI > 0 && LJ >= 2 && std::is_same<T, double>::value; }
 
+// Tetrahedra of at most this many stored entries stay in registers in
+// one-warp CTAs.
+constexpr int kRRegMax = 20;
+
 template <int LI, int LJ, int LK, int V = 0, bool HRR = false>
 struct Fast3c {
     static constexpr int L = LI + LJ + LK;
@@ -398,6 +402,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
         constexpr int NE3 = 3 * C::NE;
         constexpr int ERS = e_record<LI, LJ>();
         constexpr bool ONE = C::KS == 1;
+        constexpr bool RREG = ONE && C::NRN <= kRRegMax;
         constexpr int EPL = ONE ? (NE3 + 31) / 32 : 1;  // E values per lane
         double4 nP, nC;
         double nca = 0.0, ncc = 0.0, nE[EPL];
@@ -503,6 +508,10 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 // this warp's share of the tetrahedron by the closed form
                 // (entries are independent)
                 T Rt[L + 1], px[L + 1], py[L + 1], pz[L + 1];
+                // one-warp CTAs with a small tetrahedron keep it in registers
+                // (each lane reads only its own entries): no shared-memory
+                // store and load per entry
+                T Rr[RREG ? C::NRN : 1];
                 px[0] = py[0] = pz[0] = T(1);
 #pragma unroll
                 for (int mm = 0; mm <= L; mm++) Rt[mm] = (T)(ONE ? uRm[ONE ? mm : 0] : unit[mm * 32]);
@@ -538,7 +547,8 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                                 constexpr T h = (T)hermite_r_coef(t, mx);
                                 r = fma(h * px[2 * mx - t], ry, r);
                             });
-                            sR[(idx - C::R0) * 32 + lane] = r;
+                            if constexpr (RREG) Rr[idx - C::R0] = r;
+                            else sR[(idx - C::R0) * 32 + lane] = r;
                         });
                     }
                 });
@@ -679,7 +689,8 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                                         return false;
                                     }();
                                     if constexpr (any) {
-                                        const T r = sR[(herm_index(t + sx, u + sy, v + sz) - C::R0) * 32 + lane];
+                                        constexpr int ridx = herm_index(t + sx, u + sy, v + sz) - C::R0;
+                                        const T r = RREG ? Rr[RREG ? ridx : 0] : sR[ridx * 32 + lane];
                                         static_for<0, NC>([&](auto c_) {
                                             constexpr int c = decltype(c_)::value;
                                             constexpr double kc = ket_sph_coef(LK, c0 + c, sx, sy, sz);

@@ -58,3 +58,32 @@ class PrimitivePairData:
 
 
 PrimitivePairDataAngularList = dict  # (l_i, l_j) or l -> PrimitivePairData
+
+
+@dataclass
+class Cell:
+    """A periodic cell (reference data_structure.py:49-52): each row of
+    lattice_vectors is one lattice vector, in Bohr."""
+    dimension: int
+    lattice_vectors: np.ndarray
+
+
+@dataclass
+class Crystal:
+    """Reference data_structure.py:54-57: the cell and the atoms of one image
+    (absolute positions of an arbitrary image of each atom), with their basis
+    sets attached as for a molecule."""
+    cell: Cell
+    atoms: Molecule
+
+
+@dataclass
+class PeriodicPrimitivePair:
+    """Reference data_structure.py:59-66: a primitive pair whose j primitive
+    sits in the image cell displaced by cell_offset (3 integers) lattice vectors."""
+    i_shell: int
+    j_shell: int
+    i_primitive: int
+    j_primitive: int
+    cell_offset: np.ndarray
+    upper_bound: float

@@ -41,13 +41,18 @@ def _shell_arrays(shells):
     return ang, atom, ao, nprim, exps, coefs
 
 
-def form_primitive_pair_list(molecule: Molecule, schwarz_upper_bound: float):
-    """Return {(l_i, l_j): (i_shell, j_shell, i_prim, j_prim, bound) arrays}, sorted."""
+def form_primitive_pair_list(molecule: Molecule, schwarz_upper_bound: float, j_shift=None):
+    """Return {(l_i, l_j): (i_shell, j_shell, i_prim, j_prim, bound) arrays}, sorted.
+
+    j_shift (not in the reference; periodic images): a 3-vector in Bohr added
+    to the position of every j shell, so the pairs are (shell i in the home
+    cell, shell j in the image cell at j_shift), screened by the same rule."""
     shells = molecule.basis_shells
     if not shells or molecule.n_ao <= 0:
         raise ValueError("molecule has no orbital basis attached")
     ang, atom, ao, nprim, exps, coefs = _shell_arrays(shells)
     geom = np.asarray(molecule.geometry, dtype=np.float64)
+    geom_j = geom if j_shift is None else geom + np.asarray(j_shift, dtype=np.float64)[None, :]
     n = len(shells)
     # Per-primitive factors, as the reference forms them inside its loops.
     lf = ang[:, None].astype(np.float64)
@@ -61,8 +66,8 @@ def form_primitive_pair_list(molecule: Molecule, schwarz_upper_bound: float):
     ii, jj = ii.ravel(), jj.ravel()  # reference loop order: i_shell outer, j_shell inner
     keep = (ang[ii] < ang[jj]) | ((ang[ii] == ang[jj]) & (ao[ii] <= ao[jj]))
     ii, jj = ii[keep], jj[keep]
-    d0 = np.array([np.linalg.norm(geom[atom[a]] - geom[atom[b]]) for a, b in
-                   zip(ii, jj)]) if len(ii) < 64 else _norms(geom, atom, ii, jj)
+    d0 = np.array([np.linalg.norm(geom[atom[a]] - geom_j[atom[b]]) for a, b in
+                   zip(ii, jj)]) if len(ii) < 64 else _norms(geom, atom, ii, jj, geom_j)
 
     result = {}
     for li in np.unique(ang):
@@ -110,26 +115,29 @@ def form_primitive_pair_list(molecule: Molecule, schwarz_upper_bound: float):
     return result
 
 
-def _norms(geom, atom, ii, jj):
+def _norms(geom, atom, ii, jj, geom_j=None):
     # np.linalg.norm of a 3-vector is sqrt(dot(v, v)); evaluate it the same way
     # per unique atom pair (few), then gather.
+    geom_j = geom if geom_j is None else geom_j
     na = geom.shape[0]
     key = atom[ii] * na + atom[jj]
     uk, inv = np.unique(key, return_inverse=True)
-    vals = np.array([np.linalg.norm(geom[k // na] - geom[k % na]) for k in uk])
+    vals = np.array([np.linalg.norm(geom[k // na] - geom_j[k % na]) for k in uk])
     return vals[inv]
 
 
-def form_primitive_pair_data(molecule: Molecule, pair_list) -> dict:
-    """Pack a pair list into the (n, 4) [x, y, z, exponent] SoA tables the C ABI reads."""
+def form_primitive_pair_data(molecule: Molecule, pair_list, j_shift=None) -> dict:
+    """Pack a pair list into the (n, 4) [x, y, z, exponent] SoA tables the C ABI reads
+    (j_shift: the image offset the list was formed with, see form_primitive_pair_list)."""
     shells = molecule.basis_shells
     ang, atom, ao, nprim, exps, coefs = _shell_arrays(shells)
     geom = np.asarray(molecule.geometry, dtype=np.float64)
+    geom_j = geom if j_shift is None else geom + np.asarray(j_shift, dtype=np.float64)[None, :]
     out = {}
     for key, (si, sj, ip, jp, bnd) in pair_list.items():
         n_pair = si.shape[0]
         A = geom[atom[si]]
-        B = geom[atom[sj]]
+        B = geom_j[atom[sj]]
         a = exps[si, ip]
         b = exps[sj, jp]
         p = a + b
