@@ -943,10 +943,13 @@ def main():
     if dom:
         achieved = per_class[dom]["flops"] / (class_ms[dom] * 1e-3) / 1e12
         traffic = None
-        tfile = REPO / "profiles" / "k3c_fast_traffic.txt"
+        # DRAM bytes of one launch from an ncu capture on a small case of the
+        # same kernel, scaled to this workload by the ratio of algorithmic bytes
+        # (profiles/k3c_fast_124_traffic_small_case.md says how)
+        tfile = REPO / "profiles" / "k3c_fast_124_traffic_small_case.md"
         if tfile.exists():
             for line in tfile.read_text().splitlines():
-                if line.startswith(f"dram_bytes_per_launch {dom[0]}{dom[1]}{dom[2]} "):
+                if line.startswith(f"dram_bytes_per_launch_scaled {dom[0]}{dom[1]}{dom[2]} "):
                     traffic = float(line.split()[2])
         roof = {"bound": "fp64", "kernel": f"k3c_fast<{dom[0]},{dom[1]},{dom[2]}> (FP64)", "achieved": achieved,
                 "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": traffic,
@@ -1045,6 +1048,14 @@ def main():
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
+    # End the process here: the serving loop's worker threads and torch's
+    # cached pinned blocks would otherwise be torn down after the CUDA context
+    # at interpreter exit (an abort in a tensor destructor), failing a run
+    # whose results are already printed.
+    torch.cuda.synchronize()
+    sys.stdout.flush()
+    sys.stderr.flush()
+    os._exit(0)
 
 
 if __name__ == "__main__":

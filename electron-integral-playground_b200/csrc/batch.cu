@@ -138,9 +138,18 @@ struct eip_batch {
     bool win_charges = false;
     long long win_elems = 0;
     bool etab_ready = false;
+    // general (non-fast) classes: launched together, up to 64 classes per
+    // launch; per group its plan indices and the device work counter, and
+    // (when not too many items) a heaviest-first order of its items
+    std::vector<std::vector<int>> gen_groups;
+    int* d_gen = nullptr;              // [group][4] counters, then the orders
+    std::vector<size_t> gen_perm_off;  // per group, int2 offset into the orders (or SIZE_MAX)
     // density-fitting plan (eip_batch_df_plan): block list on the device
     DfBlock* d_df = nullptr;
-    int df_blocks = 0, df_items = 0;
+    DfGather* d_dfg = nullptr;  // the gathered c vectors of the J contraction
+    double* d_cg = nullptr;
+    int df_blocks = 0, df_items = 0, df_gathers = 0;
+    long long df_gather_elems = 0;
     long long df_ao2 = 0, df_aux = 0;  // total n_ao^2 and n_aux over the molecules
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -611,8 +620,93 @@ int eip_batch_build(eip_batch* b) {
     // heaviest classes first in the graph
     std::sort(b->plans.begin(), b->plans.end(),
               [](const ClassPlan& x, const ClassPlan& y) { return x.flops_weight > y.flops_weight; });
+    // general classes: groups of up to 64 per launch, each group's items in
+    // order of decreasing work (primitive pairs x auxiliary primitives x the
+    // class's work per unit), so that the launch does not end on a heavy item
+    {
+        std::vector<int> gen;
+        for (size_t i = 0; i < b->plans.size(); i++)
+            if (!b->plans[i].fast && b->plans[i].total_items > 0) gen.push_back((int)i);
+        for (size_t k = 0; k < gen.size(); k += 64)
+            b->gen_groups.emplace_back(gen.begin() + k, gen.begin() + std::min(gen.size(), k + 64));
+        long long gen_items = 0;
+        for (int i : gen) gen_items += b->plans[i].total_items;
+        const bool order = gen_items > 0 && gen_items <= (8LL << 20);
+        std::vector<int2> perm;
+        for (const std::vector<int>& grp : b->gen_groups) {
+            b->gen_perm_off.push_back(order ? perm.size() : SIZE_MAX);
+            if (!order) continue;
+            std::vector<std::pair<double, int2>> items;
+            for (size_t c = 0; c < grp.size(); c++) {
+                const ClassPlan& pl = b->plans[grp[c]];
+                const BraHost& B = bh[{pl.li, pl.lj}];
+                const KetHost& K = kh[pl.lk];
+                const int lk = pl.point ? 0 : pl.lk;
+                const double unit = general_item_cost(pl.li, pl.lj, lk, pl.point, b->spherical);
+                int item = 0;
+                for (int m = 0; m < b->n_mol; m++)
+                    for (int sp = B.sp_begin[m]; sp < B.sp_begin[m + 1]; sp++)
+                        for (int a = K.aux_begin[m]; a < K.aux_begin[m + 1]; a++)
+                            for (int ch = 0; ch < pl.gen_chunks; ch++) {
+                                const double w = (double)(B.begin[sp + 1] - B.begin[sp]) * (K.begin[a + 1] - K.begin[a]);
+                                items.push_back({w * unit, make_int2((int)c, item++)});
+                            }
+            }
+            std::stable_sort(items.begin(), items.end(),
+                             [](const std::pair<double, int2>& x, const std::pair<double, int2>& y) {
+                                 return x.first > y.first;
+                             });
+            for (auto& it : items) perm.push_back(it.second);
+        }
+        if (!b->gen_groups.empty()) {
+            const size_t bytes = sizeof(int) * 4 * b->gen_groups.size() + sizeof(int2) * perm.size();
+            if ((e = cudaMalloc((void**)&b->d_gen, bytes)) != cudaSuccess) return fail(b, "general work lists", e);
+            if (!perm.empty() &&
+                (e = cudaMemcpy(b->d_gen + 4 * b->gen_groups.size(), perm.data(), sizeof(int2) * perm.size(),
+                                cudaMemcpyHostToDevice)) != cudaSuccess)
+                return fail(b, "general work lists", e);
+        }
+    }
     b->built = true;
     return 0;
+}
+
+static size_t win_ob_off(int nm);
+
+// One multi-class launch per group of general classes (work maps: the plans'
+// own, or the planned window's when win is set), on the side streams.
+static int launch_general_groups(eip_batch* b, bool checksum, bool win, void* dw, double* out, int& launches) {
+    int rc = 0;
+    const int nm = b->n_mol;
+    for (size_t g = 0; g < b->gen_groups.size(); g++) {
+        std::vector<GenClassSpec> specs;
+        cudaStream_t s = b->side[g % b->side.size()];
+        for (int i : b->gen_groups[g]) {
+            ClassPlan& pl = b->plans[i];
+            cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), s);  // status word, on the launch's stream
+            BatchMap map = pl.map;
+            map.checksum = checksum ? b->d_checksum : nullptr;
+            int n_items = pl.total_items;
+            if (win) {
+                const int* v = at<int>(dw, pl.win_off);
+                map.item_begin = v;
+                map.aux_begin = v + 2 * (nm + 1);
+                map.aux_count = v + 2 * (nm + 1) + nm;
+                map.out_begin = at<long long>(dw, pl.win_off + win_ob_off(nm));
+                n_items = pl.win_items64;
+            }
+            specs.push_back(GenClassSpec{pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, pl.bra, pl.ket, map, n_items,
+                                         pl.counter + 1});
+        }
+        int* counter = b->d_gen + 4 * g;
+        const int2* perm = (!win && b->gen_perm_off[g] != SIZE_MAX)
+                               ? reinterpret_cast<const int2*>(b->d_gen + 4 * b->gen_groups.size()) + b->gen_perm_off[g]
+                               : nullptr;
+        cudaMemsetAsync(counter, 0, 4 * sizeof(int), s);
+        rc |= launch_general_multi(specs.data(), (int)specs.size(), b->spherical, perm, b->omega, out, counter, s);
+        launches++;
+    }
+    return rc;
 }
 
 long long eip_batch_output_elems(eip_batch* b) { return b && b->built ? b->out_elems : -1; }
@@ -709,13 +803,12 @@ static int capture(eip_batch* b, bool checksum) {
                                     pl.counter32, s, true);
                 launches++;
             }
-        } else {
-            BatchMap map = pl.map;
-            map.checksum = checksum ? b->d_checksum : nullptr;
-            rc |= launch_general(pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, b->spherical, pl.bra, pl.ket, map,
-                                 pl.total_items, b->omega, b->d_out, pl.counter, s);
-            launches++;
         }
+    }
+    {
+        int n = 0;
+        rc |= launch_general_groups(b, checksum, false, nullptr, b->d_out, n);
+        launches += n;
     }
     for (int i = 0; i < n_side; i++) {
         cudaEventRecord(b->events[1 + i], b->side[i]);
@@ -920,16 +1013,11 @@ int eip_batch_run_window(eip_batch* b, double* device_out, int checksum) {
                 rc |= launch_fast3c(pl.li, pl.lj, pl.lk, pl.bra, pl.ket, map, pl.win_items32, b->omega, device_out,
                                     pl.counter32, s, true);
             }
-        } else if (pl.win_items64 > 0) {
-            BatchMap map = pl.map;
-            map.item_begin = v;
-            map.aux_begin = ast;
-            map.aux_count = ast + nm;
-            map.out_begin = ob;
-            map.checksum = checksum ? b->d_checksum : nullptr;
-            rc |= launch_general(pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, b->spherical, pl.bra, pl.ket, map,
-                                 pl.win_items64, b->omega, device_out, pl.counter, s);
         }
+    }
+    {
+        int n = 0;
+        rc |= launch_general_groups(b, checksum != 0, true, dw, device_out, n);
     }
     for (int i = 0; i < n_side; i++) {
         cudaEventRecord(b->events[1 + i], b->side[i]);
@@ -998,6 +1086,7 @@ int eip_batch_df_plan(eip_batch* b, const int* n_ao, const int* n_aux) {
     OnDevice on(b);
     if (!on.ok) return fail(b, "cudaSetDevice (batch device)", cudaErrorInvalidDevice);
     const int nm = b->n_mol;
+    b->df_gather_elems = 0;
     std::vector<long long> d_off(nm + 1, 0), g_off(nm + 1, 0);
     for (int m = 0; m < nm; m++) {
         if (n_ao[m] < 0 || n_aux[m] < 0) return fail(b, "df_plan: negative size", cudaSuccess);
@@ -1014,6 +1103,8 @@ int eip_batch_df_plan(eip_batch* b, const int* n_ao, const int* n_aux) {
         }
     }
     std::vector<DfBlock> blocks;
+    std::vector<DfGather> gathers;
+    std::map<std::pair<int, int>, long long> gather_of;  // (molecule, aux class) -> cg offset
     long long items = 0;
     const int rows_per_item = df_rows_per_item();
     for (const ClassPlan& pl : b->plans) {
@@ -1029,6 +1120,14 @@ int eip_batch_df_plan(eip_batch* b, const int* n_ao, const int* n_aux) {
             bk.g_off = g_off[m];
             bk.ao = bra.grp_ao + pl.sp0[m];
             bk.aux_start = pl.ket.grp_start + pl.aux0[m];
+            auto git = gather_of.find({m, pl.lk});
+            if (git == gather_of.end()) {
+                const long long off = b->df_gather_elems;
+                gathers.push_back(DfGather{off, g_off[m], bk.aux_start, nk, pl.n_auxsh[m], off});
+                b->df_gather_elems += (long long)nk * pl.n_auxsh[m];
+                git = gather_of.emplace(std::make_pair(m, pl.lk), off).first;
+            }
+            bk.cg_off = git->second;
             bk.nsp = pl.n_sp[m];
             bk.ni = ni;
             bk.nj = nj;
@@ -1052,6 +1151,17 @@ int eip_batch_df_plan(eip_batch* b, const int* n_ao, const int* n_aux) {
     if (!blocks.empty() &&
         (e = cudaMemcpy(b->d_df, blocks.data(), sizeof(DfBlock) * blocks.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(b, "df_plan: block list upload", e);
+    if (b->d_dfg) cudaFree(b->d_dfg);
+    if (b->d_cg) cudaFree(b->d_cg);
+    b->d_dfg = nullptr;
+    b->d_cg = nullptr;
+    if ((e = cudaMalloc((void**)&b->d_dfg, sizeof(DfGather) * std::max<size_t>(gathers.size(), 1))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&b->d_cg, sizeof(double) * std::max<long long>(b->df_gather_elems, 1))) != cudaSuccess)
+        return fail(b, "df_plan: gathered vectors", e);
+    if (!gathers.empty() && (e = cudaMemcpy(b->d_dfg, gathers.data(), sizeof(DfGather) * gathers.size(),
+                                            cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(b, "df_plan: gather list upload", e);
+    b->df_gathers = (int)gathers.size();
     b->df_blocks = (int)blocks.size();
     b->df_items = (int)items;
     b->df_ao2 = d_off[nm];
@@ -1076,7 +1186,8 @@ int eip_batch_df_coulomb(eip_batch* b, const double* c, double* J) {
     if (!on.ok) return fail(b, "cudaSetDevice (batch device)", cudaErrorInvalidDevice);
     cudaError_t e = cudaMemsetAsync(J, 0, sizeof(double) * b->df_ao2, b->stream);
     if (e != cudaSuccess) return fail(b, "df_coulomb: clear", e);
-    if (launch_df_coulomb(b->d_df, b->df_blocks, b->df_items, b->d_out, c, J, b->stream) != 0)
+    if (launch_df_coulomb(b->d_df, b->df_blocks, b->df_items, b->d_dfg, b->df_gathers, b->df_gather_elems, b->d_cg,
+                          b->d_out, c, J, b->stream) != 0)
         return fail(b, "df_coulomb launch", cudaGetLastError());
     return 0;
 }
@@ -1101,6 +1212,9 @@ void eip_batch_destroy(eip_batch* b) {
     if (b->d_etab) cudaFree(b->d_etab);
     if (b->d_checksum) cudaFree(b->d_checksum);
     if (b->d_df) cudaFree(b->d_df);
+    if (b->d_dfg) cudaFree(b->d_dfg);
+    if (b->d_cg) cudaFree(b->d_cg);
+    if (b->d_gen) cudaFree(b->d_gen);
     if (b->d_win) cudaFree(b->d_win);
     if (b->h_win) cudaFreeHost(b->h_win);
     for (auto ev : b->win_uploaded)

@@ -16,8 +16,10 @@
 // kDfRows rows).  gamma: the chunk's D weights are gathered into shared
 // memory, each thread sums one column over the chunk's rows (coalesced reads
 // along the row) and adds its column total into gamma with one atomic.  J:
-// each warp reduces whole rows against c (lanes along the row, c gathered by
-// auxiliary shell) and adds the row total into J with atomics (the blocks of
+// c is first gathered into each (molecule, auxiliary class)'s column order
+// once (a small kernel); then each warp reduces whole rows against that
+// contiguous, L2-resident vector (lanes along the row) and adds the row total
+// into J with atomics (the blocks of
 // the auxiliary classes of one pair class add into the same J elements).
 #include "eip_common.cuh"
 #include "eip_internal.h"
@@ -71,9 +73,26 @@ df_gamma_kernel(const DfBlock* __restrict__ blocks, int n_blocks, int total_item
     }
 }
 
+__global__ void df_gather_kernel(const DfGather* __restrict__ gathers, int n_gathers, long long total,
+                                 const double* __restrict__ c, double* __restrict__ cg) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = n_gathers - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (gathers[mid].elem0 <= e) lo = mid;
+            else hi = mid - 1;
+        }
+        const DfGather gt = gathers[lo];
+        const int local = (int)(e - gt.elem0);
+        const int K = local / gt.nax, a = local - K * gt.nax;
+        cg[gt.cg_off + local] = c[gt.g_off + __ldg(gt.aux_start + a) + K];
+    }
+}
+
 __global__ void __launch_bounds__(kDfThreads)
 df_coulomb_kernel(const DfBlock* __restrict__ blocks, int n_blocks, int total_items,
-                  const double* __restrict__ packed, const double* __restrict__ c, double* __restrict__ Jout) {
+                  const double* __restrict__ packed, const double* __restrict__ cg, double* __restrict__ Jout) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int kWarps = kDfThreads / 32;
     for (int item = blockIdx.x; item < total_items; item += gridDim.x) {
@@ -83,15 +102,12 @@ df_coulomb_kernel(const DfBlock* __restrict__ blocks, int n_blocks, int total_it
         const long long r0 = (long long)(item - bk.item0) * kDfRows;
         const int nr = (int)min((long long)kDfRows, rows - r0);
         const int cols = bk.nk * bk.nax;
-        const double* cm = c + bk.g_off;
+        const double* cm = cg + bk.cg_off;
         for (int rr = warp; rr < nr; rr += kWarps) {
             const long long r = r0 + rr;
             const double* B = packed + bk.out_off + r * cols;
             double s = 0.0;
-            for (int K = 0; K < bk.nk; K++) {
-                const double* Bk = B + (size_t)K * bk.nax;
-                for (int a = lane; a < bk.nax; a += 32) s = fma(__ldg(Bk + a), __ldg(cm + __ldg(bk.aux_start + a) + K), s);
-            }
+            for (int col = lane; col < cols; col += 32) s = fma(__ldg(B + col), __ldg(cm + col), s);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             if (lane == 0) {
@@ -126,12 +142,19 @@ int launch_df_gamma(const DfBlock* blocks, int n_blocks, int total_items, const 
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
-int launch_df_coulomb(const DfBlock* blocks, int n_blocks, int total_items, const double* packed, const double* c,
-                      double* J, cudaStream_t s) {
+int launch_df_coulomb(const DfBlock* blocks, int n_blocks, int total_items, const DfGather* gathers, int n_gathers,
+                      long long gather_elems, double* cg, const double* packed, const double* c, double* J,
+                      cudaStream_t s) {
     if (total_items <= 0 || n_blocks <= 0) return 0;
     const int grid = df_grid(total_items);
     if (grid <= 0) return 2;
-    df_coulomb_kernel<<<grid, kDfThreads, 0, s>>>(blocks, n_blocks, total_items, packed, c, J);
+    if (gather_elems > 0) {
+        const long long gb = (gather_elems + 255) / 256;
+        df_gather_kernel<<<(unsigned)(gb < 148 * 16 ? gb : 148 * 16), 256, 0, s>>>(gathers, n_gathers, gather_elems, c,
+                                                                                  cg);
+        if (cudaGetLastError() != cudaSuccess) return 2;
+    }
+    df_coulomb_kernel<<<grid, kDfThreads, 0, s>>>(blocks, n_blocks, total_items, packed, cg, J);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 

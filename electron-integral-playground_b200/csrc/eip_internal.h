@@ -6,11 +6,10 @@
 
 #include <atomic>
 
+#include "eip_common.cuh"  // BraTable, KetTable, BatchMap (held by value below)
+
 namespace eip {
 
-struct BraTable;
-struct KetTable;
-struct BatchMap;
 
 // Per-device state.  Every device this process uses gets its own copy of the
 // constant tables (module data is per device), its own Boys-grid address and
@@ -55,6 +54,24 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
 // (lk ignored).  counter[0] must be 0 at launch; counter[1] receives a status.
 // Returns 0, 1 (unsupported class), 2 (CUDA failure) or 3 (too large).
 int general_chunks(int li, int lj, int lk, bool point, bool spherical);
+// Relative work of one item of a class (ordering items heaviest first).
+double general_item_cost(int li, int lj, int lk, bool point, bool spherical);
+// One class of a multi-class general launch: its n_items items are numbered
+// after the previous classes' (or come from perm); status: its self-check word.
+struct GenClassSpec {
+    int li, lj, lk;
+    bool point;
+    BraTable bra;
+    KetTable ket;
+    BatchMap map;
+    int n_items;
+    int* status;
+};
+// Up to 64 classes in one persistent launch; perm (optional, device) lists
+// (class, item within class) in the order the CTAs take them; counter[0]
+// must be 0 at launch.  Returns 0, 1 (unsupported class), 2 or 3 (too large).
+int launch_general_multi(const GenClassSpec* specs, int n, bool spherical, const int2* perm, double omega,
+                         double* out, int* counter, cudaStream_t s);
 int launch_general(int li, int lj, int lk, bool point, bool spherical, const BraTable& bra, const KetTable& ket,
                    const BatchMap& map, int total_items, double omega, double* out, int* counter, cudaStream_t s);
 // One packed class block of one molecule as a density-fitting matrix (df.cu):
@@ -65,15 +82,27 @@ struct DfBlock {
     long long g_off;       // the molecule's gamma / c offset (n_aux doubles per molecule)
     const int2* ao;        // the block's shell pairs: first functions (i0, j0), device
     const int* aux_start;  // the block's auxiliary shells: first function, device
+    long long cg_off;      // the block's (molecule, auxiliary class) gathered c vector
     int nsp, ni, nj, nk, nax, n_ao;
     int item0;             // first work item of the block (df_rows_per_item() rows each)
+};
+// One (molecule, auxiliary class) column vector of the J contraction:
+// cg[cg_off + K * nax + a] = c[g_off + aux_start[a] + K].
+struct DfGather {
+    long long cg_off, g_off;
+    const int* aux_start;
+    int nk, nax;
+    long long elem0;  // first element of this vector in the launch
 };
 int df_rows_per_item();
 // gamma += sum (mu nu|P) D and J += sum (mu nu|P) c over every block (device pointers).
 int launch_df_gamma(const DfBlock* blocks, int n_blocks, int total_items, const double* packed, const double* D,
                     double* gamma, cudaStream_t s);
-int launch_df_coulomb(const DfBlock* blocks, int n_blocks, int total_items, const double* packed, const double* c,
-                      double* J, cudaStream_t s);
+// J: first the c vectors are gathered into each block's column order (cg),
+// then every block row is reduced against its gathered vector.
+int launch_df_coulomb(const DfBlock* blocks, int n_blocks, int total_items, const DfGather* gathers, int n_gathers,
+                      long long gather_elems, double* cg, const double* packed, const double* c, double* J,
+                      cudaStream_t s);
 int launch_overlap_raw(int li, int lj, const BraTable& bra, const double* prim_b, double* raw, cudaStream_t s);
 int launch_transform(int li, int lj, int lk, bool spherical, int n_bra, int n_ket, const double* raw, double* out,
                      cudaStream_t s);

@@ -132,12 +132,13 @@ static GenShape general_shape(int li, int lj, int lk, bool point, bool spherical
     g.rmin = (spherical && !point) ? g.lk : 0;
     g.nr = nherm(g.L);
     g.unit_dbl = unit_ek(g) + ((!spherical && !point) ? (g.lk + 1) * (g.lk + 1) : 0);
-    // layout: unit block | closed-form coefficients | ket rows | tetrahedron
-    // decode (ints) | work region: [R | X] during the unit loop, the
-    // accumulated Cartesian block in the epilogue
+    // layout: closed-form coefficients (first: the same place for every class
+    // of a launch) | unit block | ket rows | tetrahedron decode (ints) | work
+    // region: [R | X] during the unit loop, the accumulated Cartesian block in
+    // the epilogue
     int o = 0;
-    g.o_unit = o; o += kGenUB * g.unit_dbl;
     g.o_hr = o; o += (kGenMaxL + 1) * (kGenMaxL + 1);
+    g.o_unit = o; o += kGenUB * g.unit_dbl;
     g.o_ket = o; o += g.n_ko * g.nkc;
     g.o_dec = o; o += (g.nr + 1) / 2;
     g.o_work = o;
@@ -149,58 +150,112 @@ static GenShape general_shape(int li, int lj, int lk, bool point, bool spherical
     return g;
 }
 
+// One class of a general launch: its shape, tables and work map; status is
+// its self-check word (0 ok, else the first failed check: 1 loop bound,
+// 2 molecule/pair/auxiliary index, 3 count).
+struct GenClassDesc {
+    GenShape g;
+    BraTable bra;
+    KetTable ket;
+    BatchMap map;
+    int* status;
+};
+
+// Up to kGenMaxClasses classes in one launch, passed by value in the kernel's
+// parameter space (about 23 KB): every CTA reads the descriptor of its current
+// item's class from there.  Items of class c are numbered from item0[c].
+constexpr int kGenMaxClasses = 64;
+struct GenLaunch {
+    int n_classes;
+    int item0[kGenMaxClasses + 1];
+    GenClassDesc cls[kGenMaxClasses];
+};
+
 __global__ void __launch_bounds__(kGenThreads)
-general_kernel(const double* __restrict__ boys_table, GenShape g, BraTable bra, KetTable ket, BatchMap map,
-               double omega, double* __restrict__ out, int* __restrict__ work_counter, int total_items) {
+general_kernel(const double* __restrict__ boys_table, const __grid_constant__ GenLaunch lp,
+               const int2* __restrict__ perm, double omega, double* __restrict__ out, int* __restrict__ work_counter,
+               int total_items) {
     extern __shared__ __align__(16) double gsm[];
-    double* sUnit = gsm + g.o_unit;
-    double* sHR = gsm + g.o_hr;
-    double* sKet = gsm + g.o_ket;
-    int* sDec = reinterpret_cast<int*>(gsm + g.o_dec);
-    double* sR = gsm + g.o_work;
-    double* sX = gsm + g.o_x;
-    double* sBase = gsm + g.o_base;
     __shared__ int s_item;
     const int tid = threadIdx.x;
-    // work_counter[0]: next item; work_counter[1]: status (0 ok, else the first
-    // failed self-check: 1 loop bound, 2 molecule/pair/auxiliary index, 3 count)
-    int* status = work_counter + 1;
 
-    // per-CTA tables: closed-form Hermite coefficients, spherical ket rows,
-    // tetrahedron decode (t | u << 8 | v << 16)
-    for (int e = tid; e < (kGenMaxL + 1) * (kGenMaxL + 1); e += kGenThreads) {
-        const int t = e / (kGenMaxL + 1), m = e % (kGenMaxL + 1);
-        double r = 0.0;
-        if (m >= (t + 1) / 2 && m <= t) {
-            r = 1.0;
-            for (int i = 2; i <= t; i++) r *= i;
-            for (int i = 2; i <= 2 * m - t; i++) r /= i;
-            for (int i = 2; i <= t - m; i++) r /= i;
-            for (int i = 0; i < t - m; i++) r *= 0.5;
+    // per-CTA table shared by every class: closed-form Hermite coefficients
+    // (first in every class's layout)
+    {
+        double* sHR = gsm;
+        for (int e = tid; e < (kGenMaxL + 1) * (kGenMaxL + 1); e += kGenThreads) {
+            const int t = e / (kGenMaxL + 1), m = e % (kGenMaxL + 1);
+            double r = 0.0;
+            if (m >= (t + 1) / 2 && m <= t) {
+                r = 1.0;
+                for (int i = 2; i <= t; i++) r *= i;
+                for (int i = 2; i <= 2 * m - t; i++) r /= i;
+                for (int i = 2; i <= t - m; i++) r /= i;
+                for (int i = 0; i < t - m; i++) r *= 0.5;
+            }
+            sHR[e] = r;
         }
-        sHR[e] = r;
     }
-    if (g.spherical && !g.point)
-        for (int e = tid; e < g.n_ko * g.nkc; e += kGenThreads) sKet[e] = c_sph_coef[c_sph_offset[g.lk] + e];
-    for (int N = 0; N <= g.L; N++)
-        for (int c = tid; c < ncart(N); c += kGenThreads) {
-            int x, y, z;
-            cart_decode(N, c, x, y, z);
-            sDec[nherm(N - 1) + c] = x | (y << 8) | (z << 16);
-        }
-    // accumulator entry e = tid + kGenThreads * k holds (Cartesian pair ij, ket component)
-    const int n_ent = g.nij * g.ko_chunk;
+    int cur = -1;  // class whose per-class tables are in shared memory
 
     for (int iter = 0;; iter++) {
         __syncthreads();
         if (tid == 0) s_item = atomicAdd(work_counter, 1);
         __syncthreads();
-        const int item = s_item;
-        if (item >= total_items || item < 0) return;
+        const int gitem = s_item;
+        if (gitem >= total_items || gitem < 0) return;
+        // the class of this item and its number within the class (the same
+        // for all threads of the CTA)
+        int c, item;
+        if (perm) {
+            const int2 pc = __ldg(perm + gitem);
+            c = pc.x;
+            item = pc.y;
+        } else {
+            int lo = 0, hi = lp.n_classes - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (lp.item0[mid] <= gitem) lo = mid;
+                else hi = mid - 1;
+            }
+            c = lo;
+            item = gitem - lp.item0[c];
+        }
+        if (c < 0 || c >= lp.n_classes) {
+            if (tid == 0) atomicCAS(lp.cls[0].status, 0, 2);
+            continue;
+        }
+        const GenShape& g = lp.cls[c].g;
+        const BraTable& bra = lp.cls[c].bra;
+        const KetTable& ket = lp.cls[c].ket;
+        const BatchMap& map = lp.cls[c].map;
+        int* status = lp.cls[c].status;
         if (iter > total_items) {  // a CTA can never take more items than exist
             if (tid == 0) atomicCAS(status, 0, 1);
             return;
         }
+        double* sUnit = gsm + g.o_unit;
+        const double* sHR = gsm + g.o_hr;
+        double* sKet = gsm + g.o_ket;
+        int* sDec = reinterpret_cast<int*>(gsm + g.o_dec);
+        double* sR = gsm + g.o_work;
+        double* sX = gsm + g.o_x;
+        double* sBase = gsm + g.o_base;
+        if (c != cur) {
+            // per-class tables: spherical ket rows, tetrahedron decode (t | u << 8 | v << 16)
+            if (g.spherical && !g.point)
+                for (int e = tid; e < g.n_ko * g.nkc; e += kGenThreads) sKet[e] = c_sph_coef[c_sph_offset[g.lk] + e];
+            for (int N = 0; N <= g.L; N++)
+                for (int k = tid; k < ncart(N); k += kGenThreads) {
+                    int x, y, z;
+                    cart_decode(N, k, x, y, z);
+                    sDec[nherm(N - 1) + k] = x | (y << 8) | (z << 16);
+                }
+            cur = c;
+            __syncthreads();
+        }
+        // accumulator entry e = tid + kGenThreads * k holds (Cartesian pair ij, ket component)
+        const int n_ent = g.nij * g.ko_chunk;
         int lo = 0, hi = map.n_mol - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
@@ -487,14 +542,41 @@ int general_chunks(int li, int lj, int lk, bool point, bool spherical) {
     return general_shape(li, lj, lk, point, spherical).n_chunks;
 }
 
-int launch_general(int li, int lj, int lk, bool point, bool spherical, const BraTable& bra, const KetTable& ket,
-                   const BatchMap& map, int total_items, double omega, double* out, int* counter, cudaStream_t s) {
-    if (li < 0 || li > lj || lj > kMaxAuxL || li + lj > 2 * kMaxOrbitalL || lk < 0 || lk > kMaxAuxL ||
-        li + lj + (point ? 0 : lk) > kGenMaxL)
-        return 1;
-    if (total_items <= 0) return 0;
+double general_item_cost(int li, int lj, int lk, bool point, bool spherical) {
     const GenShape g = general_shape(li, lj, lk, point, spherical);
-    const size_t smem = sizeof(double) * (size_t)g.smem_dbl;
+    // per unit: tetrahedron, ket and bra work of one chunk of ket components
+    return (double)(g.nr + g.nhb * g.ko_chunk * g.nkc / 2 + g.nij * g.ko_chunk * g.nhb / 4 + 4 * (g.L + 1));
+}
+
+static bool general_class_ok(int li, int lj, int lk, bool point) {
+    return li >= 0 && li <= lj && lj <= kMaxAuxL && li + lj <= 2 * kMaxOrbitalL && lk >= 0 && lk <= kMaxAuxL &&
+           li + lj + (point ? 0 : lk) <= kGenMaxL;
+}
+
+int launch_general_multi(const GenClassSpec* specs, int n, bool spherical, const int2* perm, double omega,
+                         double* out, int* counter, cudaStream_t s) {
+    if (n <= 0) return 0;
+    if (n > kGenMaxClasses) return 3;
+    GenLaunch lp{};
+    lp.n_classes = n;
+    size_t smem = 0;
+    long long total = 0;
+    for (int c = 0; c < n; c++) {
+        const GenClassSpec& sp = specs[c];
+        if (!general_class_ok(sp.li, sp.lj, sp.lk, sp.point)) return 1;
+        GenClassDesc& d = lp.cls[c];
+        d.g = general_shape(sp.li, sp.lj, sp.lk, sp.point, spherical);
+        d.bra = sp.bra;
+        d.ket = sp.ket;
+        d.map = sp.map;
+        d.status = sp.status;
+        lp.item0[c] = (int)total;
+        total += sp.n_items;
+        smem = std::max(smem, sizeof(double) * (size_t)d.g.smem_dbl);
+    }
+    lp.item0[n] = (int)total;
+    if (total > 0x7fffffffLL) return 3;
+    if (total == 0) return 0;
     if (smem > kGenMaxSmem) return 3;
     const double* table = boys_table_device();
     if (!table) return 2;
@@ -507,9 +589,16 @@ int launch_general(int li, int lj, int lk, bool point, bool spherical, const Bra
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, general_kernel, kGenThreads, smem) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return 2;
-    const int grid = std::min(total_items, std::max(1, per_sm) * sms);
-    general_kernel<<<grid, kGenThreads, smem, s>>>(table, g, bra, ket, map, omega, out, counter, total_items);
+    const int grid = (int)std::min<long long>(total, (long long)std::max(1, per_sm) * sms);
+    general_kernel<<<grid, kGenThreads, smem, s>>>(table, lp, perm, omega, out, counter, (int)total);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int launch_general(int li, int lj, int lk, bool point, bool spherical, const BraTable& bra, const KetTable& ket,
+                   const BatchMap& map, int total_items, double omega, double* out, int* counter, cudaStream_t s) {
+    if (!general_class_ok(li, lj, lk, point)) return 1;
+    GenClassSpec sp{li, lj, point ? 0 : lk, point, bra, ket, map, total_items, counter + 1};
+    return launch_general_multi(&sp, 1, spherical, nullptr, omega, out, counter, s);
 }
 
 // Overlap: one thread per (shell pair, ci, cj) raw Cartesian element;
