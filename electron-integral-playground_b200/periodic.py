@@ -18,10 +18,14 @@ reference library evaluated on the same lists is their oracle:
 
 Image lists: orbital pairs (shell i in the home cell, shell j in cell T) are
 screened with the front end's pair bound (pair_utility.py rule) for every T
-of the cell's images within a radius; the reference's i <= j shell order and
-its mirroring of (mu, nu) into (nu, mu) stay valid for these sums because each
-is invariant under a common translation of all images (the mirror of
-(mu_0 nu_T | P_T') is (nu_0 mu_{-T} | P_{T'-T})).  Auxiliary images are extra
+of the cell's images within a radius, in the reference's i <= j shell order
+with its mirroring of (mu, nu) into (nu, mu).  The converged sums are
+invariant under a common translation of all images (the mirror of
+(mu_0 nu_T | P_T') is (nu_0 mu_{-T} | P_{T'-T})), so there the mirroring is
+exact; with truncated image sets the result is what the reference computes on
+the same lists, and its (mu, nu) asymmetry measures how far the auxiliary
+radius is from convergence (it must reach past the pair images' centres by
+the operator's range).  Auxiliary images are extra
 primitives of the same auxiliary function (same first index), so the kernels
 contract them into one output like primitives of a contracted shell; charge
 images are extra charges whose columns are summed.
