@@ -138,8 +138,8 @@ struct eip_batch {
     bool win_charges = false;
     long long win_elems = 0;
     bool etab_ready = false;
-    // general (non-fast) classes: launched together, up to 64 classes per
-    // launch; per group its plan indices and the device work counter, and
+    // general (non-fast) classes: launched together, up to
+    // general_max_classes() per launch; per group its plan indices and the device work counter, and
     // (when not too many items) a heaviest-first order of its items
     std::vector<std::vector<int>> gen_groups;
     int* d_gen = nullptr;              // [group][4] counters, then the orders
@@ -434,10 +434,20 @@ int eip_batch_build(eip_batch* b) {
             pl.lk = ac.first;
             pl.point = ac.first == kPointKet;
             const int lk = pl.point ? 0 : pl.lk;
-            pl.fast = b->spherical && fast3c_supported(pl.li, pl.lj, lk);
-            if (!pl.fast) pl.gen_chunks = general_chunks(pl.li, pl.lj, lk, pl.point, b->spherical);
             const BraHost& B = bh[pc.first];
             const KetHost& K = kh[ac.first];
+            // The fast kernels give each lane one auxiliary shell of a tile of
+            // 32: when the molecules hold so few shells of the class that most
+            // lanes would idle (below a quarter in use), the class runs on the
+            // general kernel, which spreads one block over a whole CTA.
+            long long used = 0, slots = 0;
+            for (int m = 0; m < b->n_mol; m++) {
+                const long long nsp = B.sp_begin[m + 1] - B.sp_begin[m], nax = K.aux_begin[m + 1] - K.aux_begin[m];
+                used += nsp * nax;
+                slots += nsp * ((nax + 31) / 32) * 32;
+            }
+            pl.fast = b->spherical && fast3c_supported(pl.li, pl.lj, lk) && 4 * used >= slots;
+            if (!pl.fast) pl.gen_chunks = general_chunks(pl.li, pl.lj, lk, pl.point, b->spherical);
             const int ni = b->spherical ? nsph(pl.li) : ncart(pl.li), nj = b->spherical ? nsph(pl.lj) : ncart(pl.lj),
                       nk = b->spherical ? nsph(lk) : ncart(lk);
             long long items = 0;
@@ -620,15 +630,16 @@ int eip_batch_build(eip_batch* b) {
     // heaviest classes first in the graph
     std::sort(b->plans.begin(), b->plans.end(),
               [](const ClassPlan& x, const ClassPlan& y) { return x.flops_weight > y.flops_weight; });
-    // general classes: groups of up to 64 per launch, each group's items in
+    // general classes: groups of up to general_max_classes() per launch, each group's items in
     // order of decreasing work (primitive pairs x auxiliary primitives x the
     // class's work per unit), so that the launch does not end on a heavy item
     {
         std::vector<int> gen;
         for (size_t i = 0; i < b->plans.size(); i++)
             if (!b->plans[i].fast && b->plans[i].total_items > 0) gen.push_back((int)i);
-        for (size_t k = 0; k < gen.size(); k += 64)
-            b->gen_groups.emplace_back(gen.begin() + k, gen.begin() + std::min(gen.size(), k + 64));
+        const size_t per = (size_t)general_max_classes();
+        for (size_t k = 0; k < gen.size(); k += per)
+            b->gen_groups.emplace_back(gen.begin() + k, gen.begin() + std::min(gen.size(), k + per));
         long long gen_items = 0;
         for (int i : gen) gen_items += b->plans[i].total_items;
         const bool order = gen_items > 0 && gen_items <= (8LL << 20);

@@ -67,7 +67,8 @@ struct GenClassSpec {
     int n_items;
     int* status;
 };
-// Up to 64 classes in one persistent launch; perm (optional, device) lists
+int general_max_classes();
+// Up to general_max_classes() classes in one persistent launch; perm (optional, device) lists
 // (class, item within class) in the order the CTAs take them; counter[0]
 // must be 0 at launch.  Returns 0, 1 (unsupported class), 2 or 3 (too large).
 int launch_general_multi(const GenClassSpec* specs, int n, bool spherical, const int2* perm, double omega,

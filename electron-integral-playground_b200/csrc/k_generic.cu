@@ -162,14 +162,16 @@ struct GenClassDesc {
 };
 
 // Up to kGenMaxClasses classes in one launch, passed by value in the kernel's
-// parameter space (about 23 KB): every CTA reads the descriptor of its current
-// item's class from there.  Items of class c are numbered from item0[c].
-constexpr int kGenMaxClasses = 64;
+// parameter space (about 27 KB of the 32 KB it may hold): every CTA reads the
+// descriptor of its current item's class from there.  Items of class c are
+// numbered from item0[c].  96 covers every (l_i <= l_j <= 4 | l_k <= 5) class.
+constexpr int kGenMaxClasses = 96;
 struct GenLaunch {
     int n_classes;
     int item0[kGenMaxClasses + 1];
     GenClassDesc cls[kGenMaxClasses];
 };
+static_assert(sizeof(GenLaunch) + 64 <= 32764, "general launch descriptors exceed the kernel parameter space");
 
 __global__ void __launch_bounds__(kGenThreads)
 general_kernel(const double* __restrict__ boys_table, const __grid_constant__ GenLaunch lp,
@@ -537,6 +539,8 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
         if (map.checksum && wsum != 0.0) atomicAdd(map.checksum + m, wsum);
     }
 }
+
+int general_max_classes() { return kGenMaxClasses; }
 
 int general_chunks(int li, int lj, int lk, bool point, bool spherical) {
     return general_shape(li, lj, lk, point, spherical).n_chunks;
