@@ -280,7 +280,9 @@ def run_serving(args, torch, seed):
             pieces = sum(len(server.pieces_of(r)) for r in reqs)
         per_rate.append({"rate_rps": rate, "requests": n, "throughput_rps": st["throughput_rps"],
                          "wall_s": st["wall_s"], "latency_p50_ms": st["latency_p50_s"] * 1e3,
-                         "latency_p99_ms": st["latency_p99_s"] * 1e3, "launches": st["launches"],
+                         "latency_p99_ms": st["latency_p99_s"] * 1e3,
+                         "latency_p50_ci_ms": [x * 1e3 for x in st["latency_p50_ci_s"]],
+                         "latency_p99_ci_ms": [x * 1e3 for x in st["latency_p99_ci_s"]], "launches": st["launches"],
                          "host_s": st["host_s"]})
     del server
     torch.cuda.empty_cache()
@@ -1009,7 +1011,8 @@ def main():
                        "parallelism": f"{world} independent shard(s)"},
             "serving_summary": None if serving is None else {
                 "requests_per_rate": serving["requests"],
-                "rates": [{k: r[k] for k in ("rate_rps", "throughput_rps", "latency_p50_ms", "latency_p99_ms")}
+                "rates": [{k: r[k] for k in ("rate_rps", "throughput_rps", "latency_p50_ms", "latency_p99_ms",
+                                             "latency_p99_ci_ms")}
                           for r in serving["rates"]],
                 "alone_fp64_rps": serving["alone_fp64"]["throughput_rps"],
                 "alone_fp64_p50_ms": serving["alone_fp64"]["latency_p50_ms"]},

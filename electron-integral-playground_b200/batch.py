@@ -82,6 +82,10 @@ def _bind(L):
     L.eip_batch_upload.argtypes = [_vp]
     L.eip_batch_table_bytes.argtypes = [_vp]
     L.eip_batch_table_bytes.restype = c_ll
+    L.eip_batch_device_bytes.argtypes = [_vp]
+    L.eip_batch_device_bytes.restype = c_ll
+    L.eip_batch_class_splits.argtypes = [_vp, c_int, c_int, c_int]
+    L.eip_batch_class_splits.restype = c_int
     L.eip_batch_launches_per_run.argtypes = [_vp]
     L.eip_batch_launches_per_run.restype = ctypes.c_ulonglong
     L.eip_batch_checksums.argtypes = [_vp, _dpp]
@@ -231,6 +235,16 @@ class ThreeCenterBatch:
     @property
     def table_bytes(self):
         return int(self.L.eip_batch_table_bytes(self.h))
+
+    def class_splits(self, li, lj, lk):
+        """0: the class runs on a fast kernel; n >= 1: on the general kernel,
+        each block split into n items; -1: no such class."""
+        return int(self.L.eip_batch_class_splits(self.h, li, lj, lk))
+
+    @property
+    def device_bytes(self):
+        """Device memory held besides the output (tables, E tables, maps)."""
+        return int(self.L.eip_batch_device_bytes(self.h))
 
     @property
     def launches_per_run(self):

@@ -49,7 +49,9 @@ struct ClassPlan {
     int li, lj, lk;     // lk = kPointKet for point charges
     bool point = false;
     bool fast;
-    int gen_chunks = 1;  // general kernel (not fast): ket-component chunks per block
+    int gen_chunks = 1;  // general kernel (not fast): items per block (ket-component chunks x splits)
+    int gen_splits = 1;  // general kernel: items per (block, chunk), each over a share of the units
+    size_t split_off = 0, arrive_off = 0;  // split classes: partial blocks and arrival counters
     int total_items = 0;
     BraTable bra{};
     KetTable ket{};
@@ -113,6 +115,7 @@ struct eip_batch {
     void* h_tables = nullptr;  // pinned copy of every device table (uploaded by eip_batch_upload)
     void* d_tables = nullptr;
     size_t table_bytes = 0;
+    size_t device_bytes = 0;  // device memory of the tables, E tables, window maps and work lists
     double* d_etab = nullptr;
     double* d_out = nullptr;
     bool own_out = false;
@@ -143,6 +146,8 @@ struct eip_batch {
     // (when not too many items) a heaviest-first order of its items
     std::vector<std::vector<int>> gen_groups;
     int* d_gen = nullptr;              // [group][4] counters, then the orders
+    double* d_split = nullptr;         // partial blocks of the split general classes
+    int* d_arrive = nullptr;           // their arrival counters (0 between launches)
     std::vector<size_t> gen_perm_off;  // per group, int2 offset into the orders (or SIZE_MAX)
     // density-fitting plan (eip_batch_df_plan): block list on the device
     DfBlock* d_df = nullptr;
@@ -447,7 +452,34 @@ int eip_batch_build(eip_batch* b) {
                 slots += nsp * ((nax + 31) / 32) * 32;
             }
             pl.fast = b->spherical && fast3c_supported(pl.li, pl.lj, lk) && 4 * used >= slots;
-            if (!pl.fast) pl.gen_chunks = general_chunks(pl.li, pl.lj, lk, pl.point, b->spherical);
+            if (!pl.fast) {
+                // A general item is one CTA over every unit (primitive pair x
+                // auxiliary primitive) of its block; when a class's blocks hold
+                // many units (high-l shells of 1-8 primitives), its few heavy
+                // items would run long after the rest of the launch, so each
+                // block is split into items of about kUnitsPerSplit units.
+                const int kch = general_chunks(pl.li, pl.lj, lk, pl.point, b->spherical);
+                long long max_units = 0, base_items = 0;
+                for (int m = 0; m < b->n_mol; m++) {
+                    int max_pp = 0, max_kp = 0;
+                    for (int sp = B.sp_begin[m]; sp < B.sp_begin[m + 1]; sp++)
+                        max_pp = std::max(max_pp, B.begin[sp + 1] - B.begin[sp]);
+                    for (int a = K.aux_begin[m]; a < K.aux_begin[m + 1]; a++)
+                        max_kp = std::max(max_kp, K.begin[a + 1] - K.begin[a]);
+                    max_units = std::max(max_units, (long long)max_pp * max_kp);
+                    base_items += (long long)(B.sp_begin[m + 1] - B.sp_begin[m]) *
+                                  (K.aux_begin[m + 1] - K.aux_begin[m]) * kch;
+                }
+                constexpr int kSplitMinUnits = 64, kUnitsPerSplit = 32, kMaxSplits = 16;
+                constexpr long long kSplitScratchMax = 64LL << 20;  // doubles of partial blocks per class
+                int S = max_units >= kSplitMinUnits
+                            ? (int)std::min<long long>(kMaxSplits, (max_units + kUnitsPerSplit - 1) / kUnitsPerSplit)
+                            : 1;
+                const long long ent = general_block_entries(pl.li, pl.lj, lk, pl.point, b->spherical);
+                while (S > 1 && base_items * S * ent > kSplitScratchMax) S /= 2;
+                pl.gen_splits = S;
+                pl.gen_chunks = kch * S;
+            }
             const int ni = b->spherical ? nsph(pl.li) : ncart(pl.li), nj = b->spherical ? nsph(pl.lj) : ncart(pl.lj),
                       nk = b->spherical ? nsph(lk) : ncart(lk);
             long long items = 0;
@@ -556,6 +588,7 @@ int eip_batch_build(eip_batch* b) {
         return fail(b, "E tables", e);
     if ((e = cudaMalloc((void**)&b->d_checksum, sizeof(double) * b->n_mol)) != cudaSuccess)
         return fail(b, "checksums", e);
+    b->device_bytes += L.total + sizeof(double) * (std::max<size_t>(etab_total, 1) + b->n_mol);
     void* h = b->h_tables;
     void* d = b->d_tables;
     for (auto& kv : bh) {
@@ -620,6 +653,7 @@ int eip_batch_build(eip_batch* b) {
             return fail(b, "pinned window maps", e);
         if ((e = cudaMalloc(&b->d_win, b->win_bytes * eip_batch::kWinSlots)) != cudaSuccess)
             return fail(b, "window maps", e);
+        b->device_bytes += b->win_bytes * eip_batch::kWinSlots;
         for (int i = 0; i < eip_batch::kWinSlots; i++)
             if ((e = cudaEventCreateWithFlags(&b->win_uploaded[i], cudaEventDisableTiming)) != cudaSuccess)
                 return fail(b, "event", e);
@@ -653,7 +687,7 @@ int eip_batch_build(eip_batch* b) {
                 const BraHost& B = bh[{pl.li, pl.lj}];
                 const KetHost& K = kh[pl.lk];
                 const int lk = pl.point ? 0 : pl.lk;
-                const double unit = general_item_cost(pl.li, pl.lj, lk, pl.point, b->spherical);
+                const double unit = general_item_cost(pl.li, pl.lj, lk, pl.point, b->spherical) / pl.gen_splits;
                 int item = 0;
                 for (int m = 0; m < b->n_mol; m++)
                     for (int sp = B.sp_begin[m]; sp < B.sp_begin[m + 1]; sp++)
@@ -669,9 +703,28 @@ int eip_batch_build(eip_batch* b) {
                              });
             for (auto& it : items) perm.push_back(it.second);
         }
+        // partial blocks and arrival counters of the split classes
+        size_t split_doubles = 0, arrive_ints = 0;
+        for (int i : gen) {
+            ClassPlan& pl = b->plans[i];
+            if (pl.gen_splits <= 1) continue;
+            pl.split_off = split_doubles;
+            pl.arrive_off = arrive_ints;
+            split_doubles += (size_t)pl.total_items *
+                             general_block_entries(pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, b->spherical);
+            arrive_ints += (size_t)pl.total_items / pl.gen_splits;
+        }
+        if (split_doubles > 0) {
+            if ((e = cudaMalloc((void**)&b->d_split, sizeof(double) * split_doubles)) != cudaSuccess ||
+                (e = cudaMalloc((void**)&b->d_arrive, sizeof(int) * arrive_ints)) != cudaSuccess ||
+                (e = cudaMemset(b->d_arrive, 0, sizeof(int) * arrive_ints)) != cudaSuccess)
+                return fail(b, "general split blocks", e);
+            b->device_bytes += sizeof(double) * split_doubles + sizeof(int) * arrive_ints;
+        }
         if (!b->gen_groups.empty()) {
             const size_t bytes = sizeof(int) * 4 * b->gen_groups.size() + sizeof(int2) * perm.size();
             if ((e = cudaMalloc((void**)&b->d_gen, bytes)) != cudaSuccess) return fail(b, "general work lists", e);
+            b->device_bytes += bytes;
             if (!perm.empty() &&
                 (e = cudaMemcpy(b->d_gen + 4 * b->gen_groups.size(), perm.data(), sizeof(int2) * perm.size(),
                                 cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -683,6 +736,21 @@ int eip_batch_build(eip_batch* b) {
 }
 
 static size_t win_ob_off(int nm);
+
+// The general-launch description of a plan over `map` (n_items items); for a
+// split class also clears its arrival counters on stream s (they are left 0
+// by every complete launch; the clear keeps an interrupted one from leaking
+// into the next).
+static GenClassSpec gen_spec(eip_batch* b, ClassPlan& pl, const BatchMap& map, int n_items, cudaStream_t s) {
+    GenClassSpec sp{pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, pl.bra, pl.ket, map, n_items, pl.counter + 1};
+    if (pl.gen_splits > 1) {
+        sp.n_splits = pl.gen_splits;
+        sp.partial = b->d_split + pl.split_off;
+        sp.arrive = b->d_arrive + pl.arrive_off;
+        cudaMemsetAsync(sp.arrive, 0, sizeof(int) * (size_t)(pl.total_items / pl.gen_splits), s);
+    }
+    return sp;
+}
 
 // One multi-class launch per group of general classes (work maps: the plans'
 // own, or the planned window's when win is set), on the side streams.
@@ -706,8 +774,7 @@ static int launch_general_groups(eip_batch* b, bool checksum, bool win, void* dw
                 map.out_begin = at<long long>(dw, pl.win_off + win_ob_off(nm));
                 n_items = pl.win_items64;
             }
-            specs.push_back(GenClassSpec{pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, pl.bra, pl.ket, map, n_items,
-                                         pl.counter + 1});
+            specs.push_back(gen_spec(b, pl, map, n_items, s));
         }
         int* counter = b->d_gen + 4 * g;
         const int2* perm = (!win && b->gen_perm_off[g] != SIZE_MAX)
@@ -853,9 +920,10 @@ int eip_batch_run_class(eip_batch* b, int i_L, int j_L, int k_L) {
         if (pl.total_items == 0 && pl.total_items32 == 0) return 1;
         cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), b->stream);
         int rc = 0;
-        if (!pl.fast)
-            rc = launch_general(pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, b->spherical, pl.bra, pl.ket, pl.map,
-                                pl.total_items, b->omega, b->d_out, pl.counter, b->stream);
+        if (!pl.fast) {
+            const GenClassSpec sp = gen_spec(b, pl, pl.map, pl.total_items, b->stream);
+            rc = launch_general_multi(&sp, 1, b->spherical, nullptr, b->omega, b->d_out, pl.counter, b->stream);
+        }
         else if (pl.total_items > 0)
             rc |= pl.point ? launch_fast_point(pl.li, pl.lj, pl.bra, pl.ket, pl.map, pl.total_items, b->omega,
                                                b->d_out, pl.counter, b->stream)
@@ -1060,6 +1128,15 @@ int eip_batch_upload(eip_batch* b) {
 
 long long eip_batch_table_bytes(eip_batch* b) { return b && b->built ? (long long)b->table_bytes : -1; }
 
+long long eip_batch_device_bytes(eip_batch* b) { return b && b->built ? (long long)b->device_bytes : -1; }
+
+int eip_batch_class_splits(eip_batch* b, int i_L, int j_L, int k_L) {
+    if (!b || !b->built) return -1;
+    for (const ClassPlan& pl : b->plans)
+        if (pl.li == i_L && pl.lj == j_L && pl.lk == k_L) return pl.fast ? 0 : pl.gen_splits;
+    return -1;
+}
+
 unsigned long long eip_batch_launches_per_run(eip_batch* b) { return b ? b->launches_per_run : 0; }
 
 int eip_batch_checksums(eip_batch* b, double* host) {
@@ -1226,6 +1303,8 @@ void eip_batch_destroy(eip_batch* b) {
     if (b->d_dfg) cudaFree(b->d_dfg);
     if (b->d_cg) cudaFree(b->d_cg);
     if (b->d_gen) cudaFree(b->d_gen);
+    if (b->d_split) cudaFree(b->d_split);
+    if (b->d_arrive) cudaFree(b->d_arrive);
     if (b->d_win) cudaFree(b->d_win);
     if (b->h_win) cudaFreeHost(b->h_win);
     for (auto ev : b->win_uploaded)

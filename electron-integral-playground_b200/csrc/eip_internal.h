@@ -56,8 +56,17 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
 int general_chunks(int li, int lj, int lk, bool point, bool spherical);
 // Relative work of one item of a class (ordering items heaviest first).
 double general_item_cost(int li, int lj, int lk, bool point, bool spherical);
+// Entries of one item's Cartesian accumulator block (the partial block that a
+// split item writes).
+int general_block_entries(int li, int lj, int lk, bool point, bool spherical);
 // One class of a multi-class general launch: its n_items items are numbered
 // after the previous classes' (or come from perm); status: its self-check word.
+// n_splits > 1: every block (x chunk of ket components) is n_splits
+// consecutive items, each over its share of the block's units; they write
+// partial blocks to partial[item * general_block_entries()] and the last to
+// arrive (arrive[item / n_splits], 0 at launch and left 0) adds them in split
+// order and stores the block.  Molecule m then has
+// n_pair * n_aux * general_chunks() * n_splits items.
 struct GenClassSpec {
     int li, lj, lk;
     bool point;
@@ -66,6 +75,9 @@ struct GenClassSpec {
     BatchMap map;
     int n_items;
     int* status;
+    int n_splits = 1;
+    double* partial = nullptr;
+    int* arrive = nullptr;
 };
 int general_max_classes();
 // Up to general_max_classes() classes in one persistent launch; perm (optional, device) lists

@@ -111,6 +111,32 @@ struct Fast3c {
     }
 };
 
+// R_tuv by the closed form from R^{(m)}_000 (Rt) and the powers of PQ (px,
+// py, pz): R_tuv = sum_{mx,my,mz} h(t,mx) h(u,my) h(v,mz) X^{2mx-t} Y^{2my-u}
+// Z^{2mz-v} R^{(mx+my+mz)}_000.
+template <int t, int u, int v, typename T>
+__device__ __forceinline__ T r_closed(const T* Rt, const T* px, const T* py, const T* pz) {
+    T r = T(0);
+    static_for<(t + 1) / 2, t + 1>([&](auto mx_) {
+        constexpr int mx = decltype(mx_)::value;
+        T ry = T(0);
+        static_for<(u + 1) / 2, u + 1>([&](auto my_) {
+            constexpr int my = decltype(my_)::value;
+            T rz = T(0);
+            static_for<(v + 1) / 2, v + 1>([&](auto mz_) {
+                constexpr int mz = decltype(mz_)::value;
+                constexpr T h = (T)hermite_r_coef(v, mz);
+                rz = fma(h * pz[2 * mz - v], Rt[mx + my + mz], rz);
+            });
+            constexpr T h = (T)hermite_r_coef(u, my);
+            ry = fma(h * py[2 * my - u], rz, ry);
+        });
+        constexpr T h = (T)hermite_r_coef(t, mx);
+        r = fma(h * px[2 * mx - t], ry, r);
+    });
+    return r;
+}
+
 // Ket coefficient table of one l_k: for spherical component ko and Hermite
 // index s (|s| = LK - 2j, listed level by level in Cartesian order), the
 // combined one-centre Hermite and Cartesian->spherical coefficient; the
@@ -316,14 +342,14 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
     constexpr int L = C::L;
     constexpr int UB = C::UB;
     constexpr int NU = C::NU;
-    // dynamic shared memory (fast3c_smem_bytes): per block of UB units
+    // dynamic shared memory (Fast3c::smem_bytes): per block of UB units
     // (primitive pair x auxiliary primitive) the lanes' R^(m)_000 and unit
     // data (CTAs of several warps only), then the R tetrahedron of the current
     // unit, then the units' E tables
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sU = reinterpret_cast<double*>(smem_raw);                   // [UB][NU][32], KS > 1
     T* sR = reinterpret_cast<T*>(sU + (C::KS == 1 ? 0 : UB * NU * 32));  // [NRN][32], entries R0..NR-1
-    T* sE = sR + C::NRN * 32;                           // [UB][3 NE]
+    T* sE = sR + C::NRN * 32;                                           // [UB][3 NE]
     __shared__ int s_item;
 
     const int lane = threadIdx.x & 31;
@@ -497,29 +523,26 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 }
                 __syncthreads();
             }
-            for (int ub = 0; ub < nb; ub++) {
-                const double* unit = sU + ub * NU * 32 + lane;
-                const T* sEu = sE + ub * NE3;
-                const double X = ONE ? uX : unit[(L + 1) * 32];
-                const double Y = ONE ? uY : unit[(L + 2) * 32];
-                const double Z = ONE ? uZ : unit[(L + 3) * 32];
-                const T pref = (T)(ONE ? upref : unit[(L + 4) * 32]);
-                const double q = ONE ? uq : unit[(L + 5) * 32];
-                // this warp's share of the tetrahedron by the closed form
-                // (entries are independent)
+            // one-warp CTAs with a small tetrahedron keep it in registers
+            // (each lane reads only its own entries): no shared-memory store
+            // and load per entry
+            T Rr[RREG ? C::NRN : 1];
+            // this warp's share of unit ubr's tetrahedron by the closed form
+            // (entries are independent), into dst (or Rr)
+            auto tetra = [&](int ubr, T* dst) {
+                const double* un = sU + ubr * NU * 32 + lane;
+                const T Xr = (T)(ONE ? uX : un[(L + 1) * 32]);
+                const T Yr = (T)(ONE ? uY : un[(L + 2) * 32]);
+                const T Zr = (T)(ONE ? uZ : un[(L + 3) * 32]);
                 T Rt[L + 1], px[L + 1], py[L + 1], pz[L + 1];
-                // one-warp CTAs with a small tetrahedron keep it in registers
-                // (each lane reads only its own entries): no shared-memory
-                // store and load per entry
-                T Rr[RREG ? C::NRN : 1];
                 px[0] = py[0] = pz[0] = T(1);
 #pragma unroll
-                for (int mm = 0; mm <= L; mm++) Rt[mm] = (T)(ONE ? uRm[ONE ? mm : 0] : unit[mm * 32]);
+                for (int mm = 0; mm <= L; mm++) Rt[mm] = (T)(ONE ? uRm[ONE ? mm : 0] : un[mm * 32]);
 #pragma unroll
                 for (int mm = 1; mm <= L; mm++) {
-                    px[mm] = px[mm - 1] * (T)X;
-                    py[mm] = py[mm - 1] * (T)Y;
-                    pz[mm] = pz[mm - 1] * (T)Z;
+                    px[mm] = px[mm - 1] * Xr;
+                    py[mm] = py[mm - 1] * Yr;
+                    pz[mm] = pz[mm - 1] * Zr;
                 }
                 static_for<0, C::KS>([&](auto g) {
                     constexpr int G = decltype(g)::value;
@@ -528,30 +551,19 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                     if (warp == G) {
                         static_for<lo_e, hi_e>([&](auto e) {
                             constexpr int idx = decltype(e)::value;
-                            constexpr int t = herm_t(idx), u = herm_u(idx), v = herm_v(idx);
-                            T r = T(0);
-                            static_for<(t + 1) / 2, t + 1>([&](auto mx_) {
-                                constexpr int mx = decltype(mx_)::value;
-                                T ry = T(0);
-                                static_for<(u + 1) / 2, u + 1>([&](auto my_) {
-                                    constexpr int my = decltype(my_)::value;
-                                    T rz = T(0);
-                                    static_for<(v + 1) / 2, v + 1>([&](auto mz_) {
-                                        constexpr int mz = decltype(mz_)::value;
-                                        constexpr T h = (T)hermite_r_coef(v, mz);
-                                        rz = fma(h * pz[2 * mz - v], Rt[mx + my + mz], rz);
-                                    });
-                                    constexpr T h = (T)hermite_r_coef(u, my);
-                                    ry = fma(h * py[2 * my - u], rz, ry);
-                                });
-                                constexpr T h = (T)hermite_r_coef(t, mx);
-                                r = fma(h * px[2 * mx - t], ry, r);
-                            });
+                            const T r = r_closed<herm_t(idx), herm_u(idx), herm_v(idx)>(Rt, px, py, pz);
                             if constexpr (RREG) Rr[idx - C::R0] = r;
-                            else sR[(idx - C::R0) * 32 + lane] = r;
+                            else dst[(idx - C::R0) * 32 + lane] = r;
                         });
                     }
                 });
+            };
+            for (int ub = 0; ub < nb; ub++) {
+                const double* unit = sU + ub * NU * 32 + lane;
+                const T* sEu = sE + ub * NE3;
+                const T pref = (T)(ONE ? upref : unit[(L + 4) * 32]);
+                const double q = ONE ? uq : unit[(L + 5) * 32];
+                tetra(ub, sR);
                 // (1/2q)^{LK - j}: weight of the ket terms with |s| = LK - 2j
                 T w[LK / 2 + 1];
                 {
@@ -690,7 +702,9 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                                     }();
                                     if constexpr (any) {
                                         constexpr int ridx = herm_index(t + sx, u + sy, v + sz) - C::R0;
-                                        const T r = RREG ? Rr[RREG ? ridx : 0] : sR[ridx * 32 + lane];
+                                        T r;
+                                        if constexpr (RREG) r = Rr[ridx];
+                                        else r = sR[ridx * 32 + lane];
                                         static_for<0, NC>([&](auto c_) {
                                             constexpr int c = decltype(c_)::value;
                                             constexpr double kc = ket_sph_coef(LK, c0 + c, sx, sy, sz);

@@ -89,6 +89,7 @@ constexpr int kGenAcc = 16;   // bra accumulators per thread
 constexpr int kGenUB = 4;     // units per block
 constexpr int kGenMaxL = 21;  // 6 + 6 + 9
 constexpr size_t kGenMaxSmem = 200 * 1024;
+constexpr int kGenMaxSplits = 64;
 
 // Shape of one class for the general kernel, computed on the host.
 struct GenShape {
@@ -99,12 +100,13 @@ struct GenShape {
     int n_io, n_jo, n_ko;
     int nkc;        // Cartesian components of l_k
     int ko_chunk, n_chunks;
+    int n_splits;   // items per block and chunk, each over a share of the units (set per launch)
     int nea;        // E^{ij}_t entries per axis: (l_i+1)(l_j+1)(l_i+l_j+1)
     int rmin;       // lowest Hermite order of R the ket reads
     int nr;         // nherm(L)
     int unit_dbl;   // doubles per unit record
     // shared-memory offsets, in doubles
-    int o_unit, o_hr, o_ket, o_dec, o_work, o_x, o_base;
+    int o_unit, o_hr, o_ket, o_dec, o_row, o_work, o_x, o_base;
     int smem_dbl;
 };
 
@@ -128,6 +130,7 @@ static GenShape general_shape(int li, int lj, int lk, bool point, bool spherical
     g.nkc = ncart(g.lk);
     g.ko_chunk = std::max(1, std::min(g.n_ko, kGenThreads * kGenAcc / g.nij));
     g.n_chunks = (g.n_ko + g.ko_chunk - 1) / g.ko_chunk;
+    g.n_splits = 1;
     g.nea = (li + 1) * (lj + 1) * (g.lij + 1);
     g.rmin = (spherical && !point) ? g.lk : 0;
     g.nr = nherm(g.L);
@@ -141,6 +144,7 @@ static GenShape general_shape(int li, int lj, int lk, bool point, bool spherical
     g.o_unit = o; o += kGenUB * g.unit_dbl;
     g.o_ket = o; o += g.n_ko * g.nkc;
     g.o_dec = o; o += (g.nr + 1) / 2;
+    g.o_row = o; o += ((g.lij + 1) * (g.lij + 1) + 1) / 2;
     g.o_work = o;
     g.o_x = o + g.nr;
     g.o_base = o;
@@ -159,6 +163,8 @@ struct GenClassDesc {
     KetTable ket;
     BatchMap map;
     int* status;
+    double* partial;  // split items: partial blocks, nij * ko_chunk doubles per item
+    int* arrive;      // split items: arrivals per block and chunk
 };
 
 // Up to kGenMaxClasses classes in one launch, passed by value in the kernel's
@@ -178,7 +184,7 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
                const int2* __restrict__ perm, double omega, double* __restrict__ out, int* __restrict__ work_counter,
                int total_items) {
     extern __shared__ __align__(16) double gsm[];
-    __shared__ int s_item;
+    __shared__ int s_item, s_last;
     const int tid = threadIdx.x;
 
     // per-CTA table shared by every class: closed-form Hermite coefficients
@@ -240,6 +246,8 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
         const double* sHR = gsm + g.o_hr;
         double* sKet = gsm + g.o_ket;
         int* sDec = reinterpret_cast<int*>(gsm + g.o_dec);
+        // X is stored with v innermost: entry (t, u, v) at sRow[t (l_i+l_j+1) + u] + v
+        int* sRow = reinterpret_cast<int*>(gsm + g.o_row);
         double* sR = gsm + g.o_work;
         double* sX = gsm + g.o_x;
         double* sBase = gsm + g.o_base;
@@ -253,6 +261,19 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
                     cart_decode(N, k, x, y, z);
                     sDec[nherm(N - 1) + k] = x | (y << 8) | (z << 16);
                 }
+            {
+                const int T1 = g.lij + 1;
+                for (int e = tid; e < T1 * T1; e += kGenThreads) {
+                    const int t = e / T1, u = e - t * T1;
+                    int pos = -1;
+                    if (t + u <= g.lij) {
+                        pos = 0;
+                        for (int tt = 0; tt < t; tt++) pos += (g.lij - tt + 1) * (g.lij - tt + 2) / 2;
+                        for (int uu = 0; uu < u; uu++) pos += g.lij - t - uu + 1;
+                    }
+                    sRow[e] = pos;
+                }
+            }
             cur = c;
             __syncthreads();
         }
@@ -268,8 +289,10 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
         const int aux0 = __ldg(map.aux_begin + m);
         const int n_aux = map.aux_count ? __ldg(map.aux_count + m) : __ldg(map.aux_begin + m + 1) - aux0;
         const int local = item - __ldg(map.item_begin + m);
-        const int chunk = local % g.n_chunks;
-        const int rest = local / g.n_chunks;
+        // local = ((pair * n_aux + aux) * n_chunks + chunk) * n_splits + split
+        const int split = local % g.n_splits;
+        const int chunk = (local / g.n_splits) % g.n_chunks;
+        const int rest = local / (g.n_splits * g.n_chunks);
         const int a_local = n_aux > 0 ? rest % n_aux : 0;
         const int sp_k = n_aux > 0 ? rest / n_aux : 0;
         const int sp = __ldg(map.sp_begin + m) + sp_k;
@@ -295,8 +318,11 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
 #pragma unroll
         for (int k = 0; k < kGenAcc; k++) acc[k] = 0.0;
 
-        const int n_units = npp * nkp;
-        for (int u0 = 0; u0 < n_units; u0 += kGenUB) {
+        // this item's units: its split's share of the block's
+        const int n_all = npp * nkp;
+        const int u_begin = (int)((long long)n_all * split / g.n_splits);
+        const int n_units = (int)((long long)n_all * (split + 1) / g.n_splits);
+        for (int u0 = u_begin; u0 < n_units; u0 += kGenUB) {
             const int nb = min(kGenUB, n_units - u0);
             __syncthreads();  // the previous block's unit records are no longer read
             // (A) per unit: prefactor, Boys, R^{(m)}_000, powers; per unit and axis: E^{0 b}_t
@@ -461,7 +487,7 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
                                     x = fma(exy * ek[kz * w1 + sz], sR[herm_idx(t + sx, u + sy, v + sz)], x);
                             }
                     }
-                    sX[e] = x;
+                    sX[(sRow[t * (g.lij + 1) + u] + v) * nkoc + kl] = x;
                 }
                 __syncthreads();
                 // (3) bra: acc[(ij, k)] += pref sum_t Ex sum_u Ey sum_v Ez X[tuv][k]
@@ -487,10 +513,11 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
                                 double s = 0.0;
                                 for (int t = 0; t <= ix + jx; t++) {
                                     double su = 0.0;
+                                    const int* row = sRow + t * T1;
                                     for (int u = 0; u <= iy + jy; u++) {
                                         double sv = 0.0;
-                                        for (int v = 0; v <= iz + jz; v++)
-                                            sv = fma(ez[v], sX[herm_idx(t, u, v) * nkoc + kl], sv);
+                                        const double* xv = sX + row[u] * nkoc + kl;
+                                        for (int v = 0; v <= iz + jz; v++) sv = fma(ez[v], xv[v * nkoc], sv);
                                         su = fma(ey[u], sv, su);
                                     }
                                     s = fma(ex[t], su, s);
@@ -501,6 +528,34 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
                     }
                 }
             }
+        }
+        if (g.n_splits > 1) {
+            // Split block: write this share, count the arrival; the last split
+            // to arrive adds the shares in split order (the same sum whichever
+            // CTA is last) and goes on to the epilogue, the others take their
+            // next item.
+            double* part = lp.cls[c].partial + (size_t)item * n_ent;
+#pragma unroll
+            for (int k = 0; k < kGenAcc; k++) {
+                const int e = tid + kGenThreads * k;
+                if (e < n_ent) part[e] = acc[k];
+            }
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) s_last = atomicAdd(lp.cls[c].arrive + item / g.n_splits, 1) == g.n_splits - 1;
+            __syncthreads();
+            if (!s_last) continue;
+            __threadfence();
+            const double* first = lp.cls[c].partial + (size_t)(item - split) * n_ent;
+#pragma unroll
+            for (int k = 0; k < kGenAcc; k++) {
+                const int e = tid + kGenThreads * k;
+                double v = 0.0;
+                if (e < n_ent)
+                    for (int q = 0; q < g.n_splits; q++) v += __ldcg(first + (size_t)q * n_ent + e);
+                acc[k] = v;
+            }
+            if (tid == 0) lp.cls[c].arrive[item / g.n_splits] = 0;  // ready for the next launch
         }
         __syncthreads();
         // Epilogue: the Cartesian block to shared memory, bra (and, Cartesian,
@@ -546,6 +601,11 @@ int general_chunks(int li, int lj, int lk, bool point, bool spherical) {
     return general_shape(li, lj, lk, point, spherical).n_chunks;
 }
 
+int general_block_entries(int li, int lj, int lk, bool point, bool spherical) {
+    const GenShape g = general_shape(li, lj, lk, point, spherical);
+    return g.nij * g.ko_chunk;
+}
+
 double general_item_cost(int li, int lj, int lk, bool point, bool spherical) {
     const GenShape g = general_shape(li, lj, lk, point, spherical);
     // per unit: tetrahedron, ket and bra work of one chunk of ket components
@@ -574,6 +634,11 @@ int launch_general_multi(const GenClassSpec* specs, int n, bool spherical, const
         d.ket = sp.ket;
         d.map = sp.map;
         d.status = sp.status;
+        if (sp.n_splits < 1 || sp.n_splits > kGenMaxSplits || (sp.n_splits > 1 && (!sp.partial || !sp.arrive)))
+            return 3;
+        d.g.n_splits = sp.n_splits;
+        d.partial = sp.partial;
+        d.arrive = sp.arrive;
         lp.item0[c] = (int)total;
         total += sp.n_items;
         smem = std::max(smem, sizeof(double) * (size_t)d.g.smem_dbl);

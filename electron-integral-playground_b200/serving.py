@@ -212,7 +212,7 @@ def default_consumer(request, piece, blocks):
 class IntegralServer:
     def __init__(self, budget_bytes=150e9, precision="mixed", max_inflight=3, slice_fraction=0.25,
                  consumer=default_consumer, host_overlap=True, keep_blocks=False, fp32_threshold=None,
-                 serialize=True):
+                 serialize=True, max_resident=2, dead_bytes_max=4e9):
         import torch
 
         self.torch = torch
@@ -232,9 +232,22 @@ class IntegralServer:
         self.keep_blocks = keep_blocks
         self.kept = collections.defaultdict(dict)
         self.launches = 0
-        # finished batches: destroyed only while nothing is in flight, because
-        # freeing device memory synchronises the whole device
+        # finished batches: destroyed while nothing is in flight, because
+        # freeing device memory synchronises the whole device, or once they
+        # hold more than dead_bytes_max of device memory
         self._dead = []
+        self.dead_bytes_max = dead_bytes_max
+        self._dead_bytes = 0
+        # resident batches of windowed requests (their tables and E tables stay
+        # on the device, outside the arena, until the last window retires): at
+        # most max_resident exist or are being built; later windowed requests
+        # wait in arrival order, so a stream of large requests cannot fill the
+        # device with tables of requests whose windows are far from running
+        self.max_resident = max_resident
+        self._resident_wait = collections.deque()
+        self._n_resident = 0
+        self._dead_resident = 0
+        self.resident_high = 0  # most resident batches alive or being built at once
         # launches whose consumer work is queued: (event, off, alloc, pieces)
         self._consuming = []
         # requests whose device pieces are done, waiting for S
@@ -354,7 +367,7 @@ class IntegralServer:
                     self.host_s["plan"] += time.perf_counter() - tp
                     req.pieces_left = len(ps)
                     if req.windows_left:
-                        req.resident = builder.submit(self._build_resident, req, device)
+                        self._resident_wait.append(req)
                     waiting.extend(ps)
                     if self.host_overlap:
                         hostq.put(req)
@@ -370,13 +383,22 @@ class IntegralServer:
                         self._consuming.remove(entry)
                 if self._awaiting_s:
                     self._finish_ready(finished, t0)
-                if self._dead and ((not inflight and not self._consuming) or len(self._dead) > 64):
+                if self._resident_wait and self._n_resident >= self.max_resident and self._dead_resident:
+                    self._close_dead()  # retired resident batches make room for the next one
+                while self._resident_wait and self._n_resident < self.max_resident:
+                    req = self._resident_wait.popleft()
+                    req.resident = builder.submit(self._build_resident, req, device)
+                    self._n_resident += 1
+                    self.resident_high = max(self.resident_high, self._n_resident)
+                if self._dead and ((not inflight and not self._consuming) or len(self._dead) > 64
+                                   or self._dead_bytes > self.dead_bytes_max):
                     self._close_dead()
                 if waiting and len(inflight) < self.max_inflight:
                     largest = self.arena.largest_free
                     group, total = [], 0
                     if waiting[0].window:
-                        if waiting[0].elems + 32 <= largest:
+                        # a window runs on its request's resident batch, once that is being built
+                        if waiting[0].request.resident is not None and waiting[0].elems + 32 <= largest:
                             group.append(waiting.popleft())
                             total = group[0].elems
                     else:
@@ -414,13 +436,20 @@ class IntegralServer:
                     b = r.resident.result() if isinstance(r.resident, concurrent.futures.Future) else r.resident
                     b.close()
                     r.resident = None
+            self._resident_wait.clear()
+            self._n_resident = self._dead_resident = 0
             if self.host_overlap:
                 hostq.put(None)
                 worker.join()
         wall = time.perf_counter() - t0
         lat = np.array([r.done - r.arrival for r in finished])
+        # 95% bootstrap intervals of the percentiles (seeded resampling of the
+        # requests' latencies): the sampling spread of p50 / p99 at this size
+        boot = np.random.default_rng(0).choice(lat, size=(1000, lat.size), replace=True)
+        ci = {q: [float(x) for x in np.percentile(np.percentile(boot, q, axis=1), [2.5, 97.5])] for q in (50, 99)}
         return {"requests": n_total, "wall_s": wall, "throughput_rps": n_total / wall,
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                "latency_p50_ci_s": ci[50], "latency_p99_ci_s": ci[99],
                 "latency_mean_s": float(lat.mean()), "launches": self.launches,
                 "host_s": {k: round(v, 3) for k, v in self.host_s.items()}}
 
@@ -509,10 +538,13 @@ class IntegralServer:
             req.windows_left -= 1
             if req.windows_left == 0:  # its last window: free the tables later
                 self._dead.append(batch)
+                self._dead_bytes += batch.device_bytes
+                self._dead_resident += 1
                 req.resident = None
         else:
             batch.bind_output(0)
             self._dead.append(batch)
+            self._dead_bytes += batch.device_bytes
 
     def _consumed(self, entry, finished, t0):
         """The consumer's work on a launch's output has finished: free the arena
@@ -542,3 +574,6 @@ class IntegralServer:
             b.status()
             b.close()
         self._dead.clear()
+        self._dead_bytes = 0
+        self._n_resident -= self._dead_resident
+        self._dead_resident = 0

@@ -228,6 +228,14 @@ int eip_batch_status(eip_batch* batch);
 /* Re-copy every input table from the batch's pinned host copy to the device. */
 int eip_batch_upload(eip_batch* batch);
 long long eip_batch_table_bytes(eip_batch* batch);
+/* Device memory the built batch holds besides its output: input tables, E
+ * tables, window maps and work lists (bytes; -1 before build).  A server
+ * that keeps many batches alive budgets with it. */
+long long eip_batch_device_bytes(eip_batch* batch);
+/* How the class (i_L, j_L | k_L) runs: 0 on a fast kernel, n >= 1 on the
+ * general kernel with every block split into n items over shares of its
+ * primitive units, -1 if the batch has no such class (or is not built). */
+int eip_batch_class_splits(eip_batch* batch, int i_L, int j_L, int k_L);
 unsigned long long eip_batch_launches_per_run(eip_batch* batch);
 int eip_batch_checksums(eip_batch* batch, double* host_checksums);
 int eip_batch_copy_output(eip_batch* batch, long long offset, long long count, double* host);

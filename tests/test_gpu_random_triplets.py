@@ -97,3 +97,60 @@ def test_2000_triplets_mixed_against_fp64(triplets):
                                    atol=1e-12 * max(1.0, float(np.abs(out[0]).max())))
     f64.close()
     mix.close()
+
+
+def test_2000_triplets_batch_with_split_items(triplets):
+    """The batch splits the blocks of its heavy general classes (up to 8x8
+    primitive pairs x 8 auxiliary primitives) over several CTAs, whose partial
+    blocks the last to arrive adds in split order.  Every triplet equals the
+    unsplit drop-in (1e-12 max(1, |v|); the named cancelling triplets 1e-10),
+    and repeated runs, one class launched alone and a window over every
+    auxiliary function all reproduce the full run bit for bit."""
+    mols = [t[4] for t in triplets]
+    pds = [{t[0]: t[1]} for t in triplets]
+    ads = [{t[2]: t[3]} for t in triplets]
+    b = bt.ThreeCenterBatch(mols, pds, ads, precision="fp64")
+    b.alloc_output()
+    classes = sorted({(t[0][0], t[0][1], t[2]) for t in triplets})
+    splits = {c: b.class_splits(*c) for c in classes}
+    assert max(splits.values()) > 1, splits
+    assert splits[(4, 4, 5)] > 1
+
+    def copy():
+        buf = np.empty(b.output_elems)
+        b._check(b.L.eip_batch_copy_output(b.h, 0, b.output_elems, lib.dp(buf)), "copy")
+        return buf
+
+    b.run()
+    b.status()
+    first = copy()
+    b.run()
+    b.status()
+    np.testing.assert_array_equal(copy(), first)
+    for n, (lij, pair, lk, aux, mol) in enumerate(triplets):
+        want = mi.three_center({lij: pair}, {lk: aux}, mol)
+        scale = max(1.0, float(np.max(np.abs(want))))
+        err = float(np.max(np.abs(b.dense(n) - want))) / scale
+        assert err <= (1e-10 if n in CANCELLING_TRIPLETS else 1e-12), (n, lij, lk, err)
+    # one split class alone (over the full run's output: the same values)
+    assert b.run_class(4, 4, 5)
+    b.sync()
+    b.status()
+    np.testing.assert_array_equal(copy(), first)
+    # a window over every auxiliary function reproduces the full run
+    import torch
+
+    n = b.window()
+    assert n == b.output_elems
+    out = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+    b.run_window(out.data_ptr())
+    b.sync()
+    b.status()
+    w = out.cpu().numpy()
+    for m, (lij, pair, lk, aux, mol) in enumerate(triplets):
+        f_off, nsp, nax = b.block(m, lij[0], lij[1], lk)
+        w_off, wsp, wax = b.window_block(m, lij[0], lij[1], lk)
+        size = nsp * (2 * lij[0] + 1) * (2 * lij[1] + 1) * (2 * lk + 1) * nax
+        assert (wsp, wax) == (nsp, nax)
+        assert np.array_equal(w[w_off:w_off + size], first[f_off:f_off + size]), m
+    b.close()

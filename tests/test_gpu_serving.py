@@ -110,3 +110,27 @@ def test_server_builds_tables_when_requests_carry_molecules_only():
         for k in ka:
             scale = max(1.0, float(np.max(np.abs(ka[k]))) if ka[k].size else 1.0)
             assert float(np.max(np.abs(ka[k] - kb[k]), initial=0.0)) <= 1e-12 * scale, (r.rid, k)
+
+
+def test_resident_batches_are_bounded():
+    """Windowed requests (a 6 MB arena) keep their tables on the device in a
+    resident batch; at most max_resident such batches exist or are being
+    built at once, later ones wait in arrival order, and the results are the
+    same as with no bound (to rounding: which pieces share a launch, and so
+    whether a small class runs on the fast or the general kernel, depends on
+    admission)."""
+    reqs = _requests([6, 7, 8, 9])
+    kw = dict(budget_bytes=6e6, precision="fp64", keep_blocks=True, host_overlap=False)
+    loose = sv.IntegralServer(max_resident=8, **kw)
+    loose.serve([_fresh(r) for r in reqs], realtime=False)
+    tight = sv.IntegralServer(max_resident=1, dead_bytes_max=0, **kw)
+    tight.serve([_fresh(r) for r in reqs], realtime=False)
+    assert loose.resident_high == len(reqs)
+    assert tight.resident_high == 1
+    for r in reqs:
+        a, b = loose.kept[r.rid], tight.kept[r.rid]
+        assert a.keys() == b.keys()
+        assert any(k[0] == "3c" and k[1] > 0 for k in a), "every request should be windowed"
+        for k in a:
+            scale = max(1.0, float(np.max(np.abs(a[k]))) if a[k].size else 1.0)
+            np.testing.assert_allclose(b[k], a[k], rtol=0, atol=1e-12 * scale)
