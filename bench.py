@@ -498,7 +498,7 @@ def run_config0(seed=0):
     return out
 
 
-def run_config3(torch, bt, fp64_peak, steps=5, seed=0):
+def run_config3(torch, bt, fp64_peak, steps=5, seed=0, reference=True):
     """2000 random shell triplets (orbital l <= 4, aux l <= 5, 1-8 primitives,
     exponents log-uniform in [0.05, 1e4], centres in a 6 A cube), each its own
     molecule slot of one batch: FP64 and mixed precision, one CUDA-graph launch
@@ -548,7 +548,7 @@ def run_config3(torch, bt, fp64_peak, steps=5, seed=0):
         buf = np.empty(b.output_elems)
         b._check(b.L.eip_batch_copy_output(b.h, 0, b.output_elems, lm.dp(buf)), "copy")
         dense[prec] = (b, buf)
-    ref = oracle.reference()
+    ref = oracle.reference() if reference else None
     f64, mix = dense["fp64"][0], dense["mixed"][0]
     out["mixed_vs_fp64_max_abs"] = float(np.max(np.abs(dense["fp64"][1] - dense["mixed"][1])))
     if ref is not None:
@@ -704,6 +704,9 @@ def main():
                     help="e2e returns per-molecule checksums instead of the density-fitted J (profiling runs)")
     ap.add_argument("--no-config0", action="store_true", help="skip the 10-water per-type timings")
     ap.add_argument("--no-config3", action="store_true", help="skip the 2000 high-l random triplets")
+    ap.add_argument("--only-config3", action="store_true",
+                    help="time only the 2000 high-l random triplets (FP64 and mixed; the line's value is FP64 "
+                         "triplets/s); for profiling the general kernel")
     ap.add_argument("--no-mixed-reference", action="store_true",
                     help="skip the mixed-precision error against the reference library")
     ap.add_argument("--no-config2", action="store_true",
@@ -736,6 +739,14 @@ def main():
     if lm.lib().eip_init(local) != 0:
         raise RuntimeError(lm.lib().eip_last_error().decode())
 
+    if args.only_config3:
+        c3 = run_config3(torch, bt, bt.measure_fma_peak(), steps=args.steps, seed=args.seed, reference=False)
+        if rank == 0:
+            print(json.dumps({"metric": "random high-l shell triplets/s (FP64)", "value": c3["fp64"]["triplets_per_s"],
+                              "unit": "triplets/s", "n_gpus": 1, "steps": args.steps, "warmup": 3,
+                              "ms_per_step": c3["fp64"]["ms_per_step"], "higher_is_better": True,
+                              "config": {"workload": c3["workload"]}, "random_triplets_high_l": c3}), flush=True)
+        os._exit(0)
     mols, pds, ads, stats = build_workload(shard_seed(args.seed, rank), args.molecules)
     tot, per_class = rf.totals(stats)
     batch = bt.ThreeCenterBatch(mols, pds, ads, precision="fp64")
