@@ -837,7 +837,7 @@ def main():
                     "clocks": cs.summary(local), "launches": b.launches_per_run * args.steps,
                     "df_gamma_ms": None, "df_coulomb_ms": None, "j_abs_sum": None,
                     "h2d": b.table_bytes, "d2h": 8 * len(mols)}
-        bc = dfm.BatchCoulomb(torch, b, factors)
+        bc = dfm.BatchCoulomb(torch, b, factors, inverse_factors=True)
         J_pin = torch.empty(bc.n_ao2, dtype=torch.float64).pin_memory()
 
         def e2e_step():
@@ -864,18 +864,38 @@ def main():
         e2e = e0.elapsed_time(e1) / args.steps
         if world > 1:
             e2e = reduce_over_ranks([e2e], torch.distributed.ReduceOp.MAX, "cuda")[0]
-        # the consumer kernels alone (gamma, J) on the resident output, CUDA events
-        g0, g1, g2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        # the consumer stages alone (gamma, the solves, J) on the resident
+        # output, CUDA events; and the solves by triangular substitution
+        # (cholesky_solve) on the same gamma, for their time and difference
+        g0, g1, g2, g3, g4 = (torch.cuda.Event(enable_timing=True) for _ in range(5))
         g0.record(stream)
-        b.df_gamma(D_dev.data_ptr(), bc.gamma.data_ptr())
+        bc.fit(D_dev)
         g1.record(stream)
-        b.df_coulomb(bc.c.data_ptr(), bc.J.data_ptr())
+        bc.solve()
         g2.record(stream)
+        bc.coulomb()
+        g3.record(stream)
+        tri = dfm.BatchCoulomb(torch, b, factors, inverse_factors=False)
+        with torch.cuda.stream(stream):
+            tri.gamma.copy_(bc.gamma)
         torch.cuda.synchronize()
+        t0_ev = torch.cuda.Event(enable_timing=True)
+        t0_ev.record(stream)
+        tri.solve()
+        g4.record(stream)
+        tri.coulomb()
+        torch.cuda.synchronize()
+        c_scale = float(tri.c.abs().max())
+        j_scale = float(tri.J.abs().max())
+        solve_cmp = {"inverse_factor_ms": g1.elapsed_time(g2), "cholesky_solve_ms": t0_ev.elapsed_time(g4),
+                     "max_abs_c_diff_rel": float((bc.c - tri.c).abs().max()) / max(c_scale, 1e-300),
+                     "max_abs_J_diff_rel": float((bc.J - tri.J).abs().max()) / max(j_scale, 1e-300)}
+        del tri
         j_check = float(J_pin.abs().sum())
         return {"ms": total / args.steps, "per_step": per_step, "e2e_ms": e2e, "e2e_wall_ms": wall,
                 "clocks": cs.summary(local), "launches": b.launches_per_run * args.steps,
-                "df_gamma_ms": g0.elapsed_time(g1), "df_coulomb_ms": g1.elapsed_time(g2), "j_abs_sum": j_check,
+                "df_gamma_ms": g0.elapsed_time(g1), "df_coulomb_ms": g2.elapsed_time(g3), "j_abs_sum": j_check,
+                "df_solve": solve_cmp,
                 "h2d": b.table_bytes + 8 * D_pin.numel(), "d2h": 8 * bc.n_ao2}
 
     import tempfile
@@ -1042,14 +1062,17 @@ def main():
                     "result": "density-fitted Coulomb matrix J of every molecule (gamma = (mu nu|P) D, "
                               "c = (P|Q)^-1 gamma, J = (mu nu|P) c) copied to pinned host memory each step; "
                               "inputs per step: every pair/auxiliary table and the 64 densities, from pinned "
-                              "host memory; (P|Q) Cholesky factors made once per geometry before timing "
+                              "host memory; (P|Q) Cholesky factors and their inverses made once per geometry "
+                              "before timing (c = L^-T (L^-1 gamma))"
+                              " "
                               f"({sum(1 for x in shifts if x > 0)} of {len(shifts)} metrics needed a diagonal "
                               f"shift, largest {max(shifts, default=0):.0e} x max diag)"
                               if args.e2e_df else "per-molecule checksums (--no-e2e-df profiling run)",
                     "df_kernels_ms": None if head["df_gamma_ms"] is None else {
                         "gamma": head["df_gamma_ms"], "coulomb": head["df_coulomb_ms"], "bytes_read_each": out_bytes,
                         "gamma_gbs": out_bytes / (head["df_gamma_ms"] * 1e-3) / 1e9,
-                        "coulomb_gbs": out_bytes / (head["df_coulomb_ms"] * 1e-3) / 1e9}},
+                        "coulomb_gbs": out_bytes / (head["df_coulomb_ms"] * 1e-3) / 1e9,
+                        "solve": head.get("df_solve")}},
             "roofline": roof, "cpu_baseline": cpu, "dropin_fp64": dropin, "serving": serving,
             "water100_mixed_vs_fp64": config2, "water10_per_type": config0, "random_triplets_high_l": config3,
             "mixed_vs_reference": mixed_ref,

@@ -106,7 +106,7 @@ struct GenShape {
     int nr;         // nherm(L)
     int unit_dbl;   // doubles per unit record
     // shared-memory offsets, in doubles
-    int o_unit, o_hr, o_ket, o_dec, o_row, o_work, o_x, o_base;
+    int o_unit, o_hr, o_ket, o_kc, o_dec, o_row, o_ij, o_work, o_x, o_base;
     int smem_dbl;
 };
 
@@ -143,8 +143,10 @@ static GenShape general_shape(int li, int lj, int lk, bool point, bool spherical
     g.o_hr = o; o += (kGenMaxL + 1) * (kGenMaxL + 1);
     g.o_unit = o; o += kGenUB * g.unit_dbl;
     g.o_ket = o; o += g.n_ko * g.nkc;
+    g.o_kc = o; o += (g.n_ko * g.nkc + g.n_ko + 1) / 2;
     g.o_dec = o; o += (g.nr + 1) / 2;
     g.o_row = o; o += ((g.lij + 1) * (g.lij + 1) + 1) / 2;
+    g.o_ij = o; o += (g.nij + 1) / 2;
     g.o_work = o;
     g.o_x = o + g.nr;
     g.o_base = o;
@@ -244,17 +246,35 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
         }
         double* sUnit = gsm + g.o_unit;
         const double* sHR = gsm + g.o_hr;
+        // spherical kets: per component ko its n = sKn[ko] non-zero top-level
+        // terms, weight sKet[ko nkc + j] and code sKc[ko nkc + j] = (l_k - s_x) | s_z << 8
         double* sKet = gsm + g.o_ket;
+        int* sKc = reinterpret_cast<int*>(gsm + g.o_kc);
+        int* sKn = sKc + g.n_ko * g.nkc;
         int* sDec = reinterpret_cast<int*>(gsm + g.o_dec);
         // X is stored with v innermost: entry (t, u, v) at sRow[t (l_i+l_j+1) + u] + v
         int* sRow = reinterpret_cast<int*>(gsm + g.o_row);
+        // bra pairs in the order of their (i_x+j_x, i_y+j_y, i_z+j_z): sIJ[r] is the pair at rank r
+        int* sIJ = reinterpret_cast<int*>(gsm + g.o_ij);
         double* sR = gsm + g.o_work;
         double* sX = gsm + g.o_x;
         double* sBase = gsm + g.o_base;
         if (c != cur) {
             // per-class tables: spherical ket rows, tetrahedron decode (t | u << 8 | v << 16)
             if (g.spherical && !g.point)
-                for (int e = tid; e < g.n_ko * g.nkc; e += kGenThreads) sKet[e] = c_sph_coef[c_sph_offset[g.lk] + e];
+                for (int ko = tid; ko < g.n_ko; ko += kGenThreads) {
+                    int n = 0;
+                    for (int ck = 0; ck < g.nkc; ck++) {
+                        const double w = c_sph_coef[c_sph_offset[g.lk] + ko * g.nkc + ck];
+                        if (w == 0.0) continue;
+                        int sx, sy, sz;
+                        cart_decode(g.lk, ck, sx, sy, sz);
+                        sKet[ko * g.nkc + n] = w;
+                        sKc[ko * g.nkc + n] = (g.lk - sx) | (sz << 8);
+                        n++;
+                    }
+                    sKn[ko] = n;
+                }
             for (int N = 0; N <= g.L; N++)
                 for (int k = tid; k < ncart(N); k += kGenThreads) {
                     int x, y, z;
@@ -272,6 +292,31 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
                         for (int uu = 0; uu < u; uu++) pos += g.lij - t - uu + 1;
                     }
                     sRow[e] = pos;
+                }
+            }
+            __syncthreads();
+            {
+                // The bra loops over t <= i_x+j_x, u <= i_y+j_y, v <= i_z+j_z;
+                // ranking the pairs by that triple gives the lanes of a warp
+                // (consecutive accumulator entries) mostly the same loop shape.
+                int* sKey = reinterpret_cast<int*>(gsm + g.o_work);  // free between items
+                const int nj_c = ncart(g.lj);
+                for (int ij = tid; ij < g.nij; ij += kGenThreads) {
+                    const int ci = ij / nj_c, cj = ij - ci * nj_c;
+                    const int da = sDec[nherm(g.li - 1) + ci], db = sDec[nherm(g.lj - 1) + cj];
+                    const int sx = (da & 255) + (db & 255), sy = ((da >> 8) & 255) + ((db >> 8) & 255),
+                              sz = (da >> 16) + (db >> 16);
+                    sKey[ij] = (sx * 32 + sy) * 32 + sz;
+                }
+                __syncthreads();
+                for (int ij = tid; ij < g.nij; ij += kGenThreads) {
+                    const int key = sKey[ij];
+                    int r = 0;
+                    for (int o = 0; o < g.nij; o++) {
+                        const int ok = sKey[o];
+                        r += (ok < key) || (ok == key && o < ij);
+                    }
+                    sIJ[r] = ij;
                 }
             }
             cur = c;
@@ -467,13 +512,17 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
                     if (g.point) {
                         x = sR[h];
                     } else if (g.spherical) {
-                        const double* row = sKet + ko * g.nkc;
-                        const int first = nherm(g.lk - 1);
-                        for (int c = 0; c < g.nkc; c++) {
-                            const double w = row[c];
-                            if (w == 0.0) continue;
-                            const int dc = sDec[first + c];
-                            x = fma(w, sR[herm_idx(t + (dc & 255), u + ((dc >> 8) & 255), v + (dc >> 16))], x);
+                        // R index of h + s, |s| = l_k: order N = |h| + l_k, so
+                        // herm_idx = nherm(N-1) + m (m+1) / 2 + v + s_z with
+                        // m = N - (t + s_x) = u + v + l_k - s_x
+                        const double* w = sKet + ko * g.nkc;
+                        const int* code = sKc + ko * g.nkc;
+                        const int N = t + u + v + g.lk;
+                        const int base = N * (N + 1) * (N + 2) / 6 + v, q = u + v;
+                        for (int j = 0; j < sKn[ko]; j++) {
+                            const int cd = code[j];
+                            const int mm = q + (cd & 255);
+                            x = fma(w[j], sR[base + ((mm * (mm + 1)) >> 1) + (cd >> 8)], x);
                         }
                     } else {
                         int kx, ky, kz;
@@ -500,7 +549,8 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
                     for (int k = 0; k < kGenAcc; k++) {
                         const int e = tid + kGenThreads * k;
                         if (e < n_ent) {
-                            const int ij = e / g.ko_chunk, kl = e - ij * g.ko_chunk;
+                            const int rk = e / g.ko_chunk, kl = e - rk * g.ko_chunk;
+                            const int ij = sIJ[rk];
                             if (kl < nkoc) {
                                 const int ci = ij / ncart(g.lj), cj = ij - ci * ncart(g.lj);
                                 const int da = sDec[nherm(g.li - 1) + ci], db = sDec[nherm(g.lj - 1) + cj];
@@ -563,7 +613,10 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
 #pragma unroll
         for (int k = 0; k < kGenAcc; k++) {
             const int e = tid + kGenThreads * k;
-            if (e < n_ent) sBase[e] = acc[k];
+            if (e < n_ent) {
+                const int rk = e / g.ko_chunk;
+                sBase[sIJ[rk] * g.ko_chunk + (e - rk * g.ko_chunk)] = acc[k];
+            }
         }
         __syncthreads();
         const size_t obase = (size_t)__ldg(map.out_begin + m);

@@ -171,17 +171,29 @@ class BatchCoulomb:
 
         gamma = (mu nu|P) D,   c = (P|Q)^{-1} gamma,   J = (mu nu|P) c
 
-    ``metric_factors``: per molecule the lower Cholesky factor of its (P|Q)
-    (device, FP64), e.g. ``torch.linalg.cholesky(metric_matrix(...))``.  The
-    densities and results are concatenated device arrays (molecule m's n_ao^2
-    block after the previous molecules'); ``run`` queues everything on the
-    batch stream's side of the current torch stream and returns J."""
+    ``metric_factors``: per molecule the lower Cholesky factor L of its (P|Q)
+    (device, FP64), e.g. ``torch.linalg.cholesky(metric_matrix(...))``.  With
+    ``inverse_factors`` the factors are inverted once here (L^{-1}, a
+    triangular solve against the identity, like the factorisation a
+    per-geometry cost) and every solve is two matrix-vector products,
+    c = L^{-T} (L^{-1} gamma), each reading the inverse once at memory speed;
+    otherwise each solve is a pair of triangular substitutions
+    (``torch.cholesky_solve``).  The densities and results are concatenated
+    device arrays (molecule m's n_ao^2 block after the previous molecules');
+    ``run`` queues everything on the batch stream's side of the current torch
+    stream and returns J."""
 
-    def __init__(self, torch, batch, metric_factors):
+    def __init__(self, torch, batch, metric_factors, inverse_factors=False):
         self.torch = torch
         self.batch = batch
         self.n_ao2, self.n_aux = batch.df_plan()
-        self.factors = list(metric_factors)
+        self.inverse = inverse_factors
+        self.factors = []
+        for Lf in metric_factors:
+            if inverse_factors:
+                eye = torch.eye(Lf.shape[0], dtype=Lf.dtype, device=Lf.device)
+                Lf = torch.linalg.solve_triangular(Lf, eye, upper=False)
+            self.factors.append(Lf)
         self.aux_off = np.concatenate([[0], np.cumsum([m.n_aux for m in batch.molecules])]).astype(np.int64)
         self.ao_off = np.concatenate([[0], np.cumsum([m.n_ao ** 2 for m in batch.molecules])]).astype(np.int64)
         dev = "cuda"
@@ -190,17 +202,36 @@ class BatchCoulomb:
         self.J = torch.zeros(max(self.n_ao2, 1), dtype=torch.float64, device=dev)
         self.stream = torch.cuda.ExternalStream(batch.stream)
 
+    def fit(self, D):
+        """gamma = (mu nu|P) D for every molecule (D: concatenated densities)."""
+        self.batch.df_gamma(D.data_ptr(), self.gamma.data_ptr())
+
+    def solve(self):
+        """c = (P|Q)^{-1} gamma for every molecule, on the batch stream."""
+        torch = self.torch
+        with torch.cuda.stream(self.stream):
+            for m, F in enumerate(self.factors):
+                a0, a1 = int(self.aux_off[m]), int(self.aux_off[m + 1])
+                if a1 <= a0:
+                    continue
+                if self.inverse:
+                    self.c[a0:a1] = torch.mv(F.T, torch.mv(F, self.gamma[a0:a1]))
+                else:
+                    self.c[a0:a1] = torch.cholesky_solve(self.gamma[a0:a1, None], F)[:, 0]
+
+    def coulomb(self):
+        """J = (mu nu|P) c for every molecule."""
+        self.batch.df_coulomb(self.c.data_ptr(), self.J.data_ptr())
+
     def run(self, D):
         """D: concatenated densities (device tensor of n_ao2 doubles).  Returns
-        the concatenated J (device tensor; valid once the batch stream is done)."""
-        torch = self.torch
-        self.batch.df_gamma(D.data_ptr(), self.gamma.data_ptr())
-        with torch.cuda.stream(self.stream):
-            for m, Lf in enumerate(self.factors):
-                a0, a1 = int(self.aux_off[m]), int(self.aux_off[m + 1])
-                if a1 > a0:
-                    self.c[a0:a1] = torch.cholesky_solve(self.gamma[a0:a1, None], Lf)[:, 0]
-        self.batch.df_coulomb(self.c.data_ptr(), self.J.data_ptr())
+        the concatenated J (device tensor; valid once the batch stream is done).
+        The batch stream first waits for the current torch stream, where D and
+        this object's buffers and (inverted) factors were made."""
+        self.stream.wait_stream(self.torch.cuda.current_stream())
+        self.fit(D)
+        self.solve()
+        self.coulomb()
         return self.J
 
     def molecule_J(self, m):

@@ -89,4 +89,11 @@ def test_batch_coulomb_kernels_match_dense():
         np.testing.assert_allclose(Jk, J_ref, rtol=0, atol=1e-12 * max(1.0, np.abs(J_ref).max()))
         J1, c1, _ = df.coulomb_matrix(m, pd, ad, Dm)
         np.testing.assert_allclose(Jk, J1.cpu().numpy(), rtol=0, atol=1e-9 * max(1.0, np.abs(J_ref).max()))
+    # solves through the inverted factors (two matrix-vector products) give the
+    # same J as the triangular substitutions
+    inv = df.BatchCoulomb(torch, b, factors, inverse_factors=True)
+    inv.run(D)
+    b.sync()
+    Jt, Ji = bc.J.cpu().numpy(), inv.J.cpu().numpy()
+    np.testing.assert_allclose(Ji, Jt, rtol=0, atol=1e-10 * max(1.0, np.abs(Jt).max()))
     b.close()
