@@ -147,6 +147,8 @@ struct eip_batch {
     std::vector<std::vector<int>> gen_groups;
     int* d_gen = nullptr;              // [group][4] counters, then the orders
     double* d_split = nullptr;         // partial blocks of the split general classes
+    double* d_gen_etab = nullptr;      // E tables of the pair classes that general classes use
+    std::map<std::pair<int, int>, size_t> gen_etab_offset;
     int* d_arrive = nullptr;           // their arrival counters (0 between launches)
     std::vector<size_t> gen_perm_off;  // per group, int2 offset into the orders (or SIZE_MAX)
     // density-fitting plan (eip_batch_df_plan): block list on the device
@@ -703,6 +705,21 @@ int eip_batch_build(eip_batch* b) {
                              });
             for (auto& it : items) perm.push_back(it.second);
         }
+        // E tables of the pair classes the general classes use (computed with
+        // the fast classes' tables at every run)
+        size_t gen_etab_doubles = 0;
+        for (int i : gen) {
+            const ClassPlan& pl = b->plans[i];
+            const std::pair<int, int> pc{pl.li, pl.lj};
+            if (b->gen_etab_offset.count(pc)) continue;
+            b->gen_etab_offset[pc] = gen_etab_doubles;
+            gen_etab_doubles += (size_t)general_e_doubles(pl.li, pl.lj) * bh[pc].P.size();
+        }
+        if (gen_etab_doubles > 0) {
+            if ((e = cudaMalloc((void**)&b->d_gen_etab, sizeof(double) * gen_etab_doubles)) != cudaSuccess)
+                return fail(b, "general E tables", e);
+            b->device_bytes += sizeof(double) * gen_etab_doubles;
+        }
         // partial blocks and arrival counters of the split classes
         size_t split_doubles = 0, arrive_ints = 0;
         for (int i : gen) {
@@ -741,8 +758,22 @@ static size_t win_ob_off(int nm);
 // split class also clears its arrival counters on stream s (they are left 0
 // by every complete launch; the clear keeps an interrupted one from leaking
 // into the next).
+// The general kernel's E tables of every pair class a general class uses,
+// on stream s (after the tables' upload, before the general launches).
+static int launch_gen_etabs(eip_batch* b, cudaStream_t s, unsigned long long* launches = nullptr) {
+    int rc = 0;
+    for (const auto& kv : b->gen_etab_offset) {
+        rc |= launch_general_e_table(kv.first.first, kv.first.second, b->bra_by_class[kv.first],
+                                     b->d_gen_etab + kv.second, s);
+        if (launches) ++*launches;
+    }
+    return rc;
+}
+
 static GenClassSpec gen_spec(eip_batch* b, ClassPlan& pl, const BatchMap& map, int n_items, cudaStream_t s) {
     GenClassSpec sp{pl.li, pl.lj, pl.point ? 0 : pl.lk, pl.point, pl.bra, pl.ket, map, n_items, pl.counter + 1};
+    auto et = b->gen_etab_offset.find({pl.li, pl.lj});
+    if (et != b->gen_etab_offset.end()) sp.etab = b->d_gen_etab + et->second;
     if (pl.gen_splits > 1) {
         sp.n_splits = pl.gen_splits;
         sp.partial = b->d_split + pl.split_off;
@@ -858,6 +889,7 @@ static int capture(eip_batch* b, bool checksum) {
                              b->stream);
         launches++;
     }
+    rc |= launch_gen_etabs(b, b->stream, &launches);
     cudaEventRecord(b->events[0], b->stream);
     for (int i = 0; i < n_side; i++) cudaStreamWaitEvent(b->side[i], b->events[0], 0);
     int next = 0;
@@ -921,8 +953,11 @@ int eip_batch_run_class(eip_batch* b, int i_L, int j_L, int k_L) {
         cudaMemsetAsync(pl.counter, 0, 4 * sizeof(int), b->stream);
         int rc = 0;
         if (!pl.fast) {
+            auto et = b->gen_etab_offset.find({pl.li, pl.lj});
+            if (et != b->gen_etab_offset.end())
+                rc |= launch_general_e_table(pl.li, pl.lj, pl.bra, b->d_gen_etab + et->second, b->stream);
             const GenClassSpec sp = gen_spec(b, pl, pl.map, pl.total_items, b->stream);
-            rc = launch_general_multi(&sp, 1, b->spherical, nullptr, b->omega, b->d_out, pl.counter, b->stream);
+            rc |= launch_general_multi(&sp, 1, b->spherical, nullptr, b->omega, b->d_out, pl.counter, b->stream);
         }
         else if (pl.total_items > 0)
             rc |= pl.point ? launch_fast_point(pl.li, pl.lj, pl.bra, pl.ket, pl.map, pl.total_items, b->omega,
@@ -1056,6 +1091,7 @@ int eip_batch_run_window(eip_batch* b, double* device_out, int checksum) {
             rc |= launch_e_table(kv.first.first, kv.first.second, kv.second, b->d_etab + b->etab_offset[kv.first],
                                  b->stream);
         }
+        rc |= launch_gen_etabs(b, b->stream);
         b->etab_ready = true;
     }
     if (checksum) cudaMemsetAsync(b->d_checksum, 0, sizeof(double) * nm, b->stream);
@@ -1304,6 +1340,7 @@ void eip_batch_destroy(eip_batch* b) {
     if (b->d_cg) cudaFree(b->d_cg);
     if (b->d_gen) cudaFree(b->d_gen);
     if (b->d_split) cudaFree(b->d_split);
+    if (b->d_gen_etab) cudaFree(b->d_gen_etab);
     if (b->d_arrive) cudaFree(b->d_arrive);
     if (b->d_win) cudaFree(b->d_win);
     if (b->h_win) cudaFreeHost(b->h_win);

@@ -17,10 +17,11 @@
 // memory, each thread sums one column over the chunk's rows (coalesced reads
 // along the row) and adds its column total into gamma with one atomic.  J:
 // c is first gathered into each (molecule, auxiliary class)'s column order
-// once (a small kernel); then each warp reduces whole rows against that
-// contiguous, L2-resident vector (lanes along the row) and adds the row total
-// into J with atomics (the blocks of
-// the auxiliary classes of one pair class add into the same J elements).
+// once (a small kernel); then each warp reduces four consecutive rows at a
+// time against that contiguous, L2-resident vector (lanes along the rows, one
+// load of c per column for the four) and adds the row totals into J with
+// atomics (the blocks of the auxiliary classes of one pair class add into the
+// same J elements).
 #include "eip_common.cuh"
 #include "eip_internal.h"
 
@@ -28,6 +29,7 @@ namespace eip {
 
 constexpr int kDfThreads = 256;
 constexpr int kDfRows = 32;
+constexpr int kDfRowsPerWarp = 4;  // J: rows a warp reduces together (kDfRows = 8 warps x 4)
 
 __device__ __forceinline__ int df_block_of(const DfBlock* __restrict__ blocks, int n_blocks, int item) {
     int lo = 0, hi = n_blocks - 1;
@@ -103,21 +105,39 @@ df_coulomb_kernel(const DfBlock* __restrict__ blocks, int n_blocks, int total_it
         const int nr = (int)min((long long)kDfRows, rows - r0);
         const int cols = bk.nk * bk.nax;
         const double* cm = cg + bk.cg_off;
-        for (int rr = warp; rr < nr; rr += kWarps) {
+        // each warp takes kDfRowsPerWarp consecutive rows at once: one load of
+        // c per column feeds every row, and the rows' loads are in flight together
+        for (int rr = warp * kDfRowsPerWarp; rr < nr; rr += kWarps * kDfRowsPerWarp) {
             const long long r = r0 + rr;
             const double* B = packed + bk.out_off + r * cols;
-            double s = 0.0;
-            for (int col = lane; col < cols; col += 32) s = fma(__ldg(B + col), __ldg(cm + col), s);
+            const int nq = min(kDfRowsPerWarp, nr - rr);
+            double s[kDfRowsPerWarp];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) {
-                const int sp = (int)(r / nij), ij = (int)(r - (long long)sp * nij);
+            for (int q = 0; q < kDfRowsPerWarp; q++) s[q] = 0.0;
+            for (int col = lane; col < cols; col += 32) {
+                const double cv = __ldg(cm + col);
+#pragma unroll
+                for (int q = 0; q < kDfRowsPerWarp; q++)
+                    if (q < nq) s[q] = fma(__ldg(B + (size_t)q * cols + col), cv, s[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < kDfRowsPerWarp; q++)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+            // lane q adds row q into J (and its mirror)
+            double mine = 0.0;
+#pragma unroll
+            for (int q = 0; q < kDfRowsPerWarp; q++)
+                if (lane == q) mine = s[q];
+            if (lane < nq) {
+                const long long rq = r + lane;
+                const int sp = (int)(rq / nij), ij = (int)(rq - (long long)sp * nij);
                 const int I = ij / bk.nj, J = ij - I * bk.nj;
                 const int2 ao = bk.ao[sp];
                 double* Jm = Jout + bk.d_off;
                 const size_t mu = (size_t)ao.x + I, nu = (size_t)ao.y + J;
-                atomicAdd(Jm + mu * bk.n_ao + nu, s);
-                if (ao.x != ao.y) atomicAdd(Jm + nu * bk.n_ao + mu, s);
+                atomicAdd(Jm + mu * bk.n_ao + nu, mine);
+                if (ao.x != ao.y) atomicAdd(Jm + nu * bk.n_ao + mu, mine);
             }
         }
     }

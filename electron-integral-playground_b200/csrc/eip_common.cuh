@@ -189,6 +189,16 @@ __device__ __forceinline__ void boys(const double* __restrict__ table, double T,
     }
 }
 
+// 1/n for n = 0..2 kMaxBoysM + 1 (entry 0 unused): the run-time variant's
+// recursion factors as multiplications, the same as the compile-time variant.
+#define EIP_INV8(n) 1.0 / (n), 1.0 / (n + 1), 1.0 / (n + 2), 1.0 / (n + 3), 1.0 / (n + 4), 1.0 / (n + 5), \
+                    1.0 / (n + 6), 1.0 / (n + 7)
+static __constant__ double c_inv_n[48] = {0.0,        1.0,        0.5,        1.0 / 3,    0.25,       0.2,
+                                          1.0 / 6,    1.0 / 7,    EIP_INV8(8), EIP_INV8(16), EIP_INV8(24),
+                                          EIP_INV8(32), EIP_INV8(40)};
+#undef EIP_INV8
+static_assert(2 * kMaxBoysM + 1 < 48, "reciprocal table too short");
+
 // Run-time order variant (generic kernels).
 __device__ __forceinline__ void boys_rt(const double* __restrict__ table, int L, double T, double* F) {
     const double eT = exp(-T);
@@ -197,9 +207,9 @@ __device__ __forceinline__ void boys_rt(const double* __restrict__ table, int L,
         const double d = T - i * kBoysStep;
         const double* row = table + i * kBoysOrders + L;
         double acc = __ldg(row + kBoysTaylor - 1);
-        for (int k = kBoysTaylor - 1; k >= 1; k--) acc = fma(-d / k, acc, __ldg(row + k - 1));
+        for (int k = kBoysTaylor - 1; k >= 1; k--) acc = fma(-d * c_inv_n[k], acc, __ldg(row + k - 1));
         F[L] = acc;
-        for (int m = L - 1; m >= 0; m--) F[m] = fma(2.0 * T, F[m + 1], eT) / (2 * m + 1);
+        for (int m = L - 1; m >= 0; m--) F[m] = fma(2.0 * T, F[m + 1], eT) * c_inv_n[2 * m + 1];
     } else {
         F[0] = 0.88622692545275801365 * sqrt(1.0 / T);
         for (int m = 0; m < L; m++) F[m + 1] = fma((double)(2 * m + 1), F[m], -eT) * (0.5 / T);

@@ -56,6 +56,10 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
 int general_chunks(int li, int lj, int lk, bool point, bool spherical);
 // Relative work of one item of a class (ordering items heaviest first).
 double general_item_cost(int li, int lj, int lk, bool point, bool spherical);
+// E tables of pair class (li, lj) for the general kernel (GenClassSpec::etab):
+// general_e_doubles(li, lj) doubles per primitive pair of the bra table.
+int general_e_doubles(int li, int lj);
+int launch_general_e_table(int li, int lj, const BraTable& bra, double* out, cudaStream_t s);
 // Entries of one item's Cartesian accumulator block (the partial block that a
 // split item writes).
 int general_block_entries(int li, int lj, int lk, bool point, bool spherical);
@@ -78,6 +82,7 @@ struct GenClassSpec {
     int n_splits = 1;
     double* partial = nullptr;
     int* arrive = nullptr;
+    const double* etab = nullptr;  // E tables per primitive pair, or nullptr (computed in the kernel)
 };
 int general_max_classes();
 // Up to general_max_classes() classes in one persistent launch; perm (optional, device) lists

@@ -110,6 +110,34 @@ struct GenShape {
     int smem_dbl;
 };
 
+// E^{ij}_t along one axis for every i <= l_i, j <= l_j, at E[(i (l_j+1) + j)(l_i+l_j+1) + t]:
+// E^{i+1,0}_t = E^{i,0}_{t-1} / (2p) + PA E^{i,0}_t + (t+1) E^{i,0}_{t+1} for
+// i < l_i + l_j, then E^{i,j+1}_t = E^{i+1,j}_t + AB E^{i,j}_t, level j kept in
+// W (rows i <= l_i + l_j - j) and rows i <= l_i stored
+// (c_library/mcmurchie_davidson_E_term.hpp:22-45, 166-199).
+__device__ void general_e_axis(int li, int lj, double pa_d, double ab_d, double inv2p, double* E) {
+    const int N = li + lj, T1 = li + lj + 1;
+    double W[kMaxOrbitalL * 2 + 1][kMaxOrbitalL * 2 + 1];
+    for (int i = 0; i <= N; i++)
+        for (int t = 0; t <= N; t++) W[i][t] = 0.0;
+    W[0][0] = 1.0;
+    for (int i = 0; i < N; i++)
+        for (int t = 0; t <= i + 1; t++) {
+            double v = 0.0;
+            if (t >= 1) v = inv2p * W[i][t - 1];
+            if (t <= i) v = fma(pa_d, W[i][t], v);
+            if (t + 1 <= i) v = fma((double)(t + 1), W[i][t + 1], v);
+            W[i + 1][t] = v;
+        }
+    for (int j = 0; j <= lj; j++) {
+        for (int i = 0; i <= li; i++)
+            for (int t = 0; t <= N; t++) E[(i * (lj + 1) + j) * T1 + t] = W[i][t];
+        if (j == lj) break;
+        for (int i = 0; i + j + 1 <= N; i++)
+            for (int t = 0; t <= N; t++) W[i][t] = fma(ab_d, W[i][t], W[i + 1][t]);
+    }
+}
+
 // Unit record: [0, L] R^{(m)}_000 (-2 zeta)^m; L+1 prefactor; then X, Y, Z
 // powers (L+1 each); then E^{ij}_t for x, y, z (nea each, index
 // (i (l_j+1) + j)(l_i+l_j+1) + t); then, Cartesian
@@ -165,6 +193,7 @@ struct GenClassDesc {
     KetTable ket;
     BatchMap map;
     int* status;
+    const double* etab;  // optional: E tables per primitive pair (general_e_table_kernel)
     double* partial;  // split items: partial blocks, nij * ko_chunk doubles per item
     int* arrive;      // split items: arrivals per block and chunk
 };
@@ -356,6 +385,7 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
             continue;
         }
         const double4 AB = bra.grp_AB[sp];
+        const double* etab = lp.cls[c].etab;  // per primitive pair E tables, or computed here
         const int ko0 = chunk * g.ko_chunk;
         const int nkoc = min(g.ko_chunk, g.n_ko - ko0);
 
@@ -371,7 +401,7 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
             const int nb = min(kGenUB, n_units - u0);
             __syncthreads();  // the previous block's unit records are no longer read
             // (A) per unit: prefactor, Boys, R^{(m)}_000, powers; per unit and axis: E^{0 b}_t
-            for (int w = tid; w < 4 * nb; w += kGenThreads) {
+            for (int w = tid; w < (etab ? nb : 4 * nb); w += kGenThreads) {
                 const int ub = w < nb ? w : (w - nb) / 3;
                 const int u = u0 + ub;
                 const int pp = pb + u / nkp, kp = kb + u % nkp;
@@ -444,35 +474,20 @@ general_kernel(const double* __restrict__ boys_table, const __grid_constant__ Ge
                         pz *= Z;
                     }
                 } else {
-                    // E^{i+1,0}_t = E^{i,0}_{t-1} / (2p) + PA E^{i,0}_t + (t+1) E^{i,0}_{t+1}
-                    // for i < l_i + l_j, then E^{i,j+1}_t = E^{i+1,j}_t + AB E^{i,j}_t,
-                    // level j kept in W (rows i <= l_i + l_j - j) and rows i <= l_i stored
                     const int d = (w - nb) % 3;
                     const double4 PA = bra.prim_PA[pp];
                     const double pa_d = d == 0 ? PA.x : (d == 1 ? PA.y : PA.z);
                     const double ab_d = d == 0 ? AB.x : (d == 1 ? AB.y : AB.z);
-                    const double inv2p = 0.5 / P.w;
-                    const int N = g.lij, T1 = g.lij + 1;
-                    double* E = U + unit_e(g) + d * g.nea;
-                    double W[kMaxOrbitalL * 2 + 1][kMaxOrbitalL * 2 + 1];
-                    for (int i = 0; i <= N; i++)
-                        for (int t = 0; t <= N; t++) W[i][t] = 0.0;
-                    W[0][0] = 1.0;
-                    for (int i = 0; i < N; i++)
-                        for (int t = 0; t <= i + 1; t++) {
-                            double v = 0.0;
-                            if (t >= 1) v = inv2p * W[i][t - 1];
-                            if (t <= i) v = fma(pa_d, W[i][t], v);
-                            if (t + 1 <= i) v = fma((double)(t + 1), W[i][t + 1], v);
-                            W[i + 1][t] = v;
-                        }
-                    for (int j = 0; j <= g.lj; j++) {
-                        for (int i = 0; i <= g.li; i++)
-                            for (int t = 0; t <= N; t++) E[(i * (g.lj + 1) + j) * T1 + t] = W[i][t];
-                        if (j == g.lj) break;
-                        for (int i = 0; i + j + 1 <= N; i++)
-                            for (int t = 0; t <= N; t++) W[i][t] = fma(ab_d, W[i][t], W[i + 1][t]);
-                    }
+                    general_e_axis(g.li, g.lj, pa_d, ab_d, 0.5 / P.w, U + unit_e(g) + d * g.nea);
+                }
+            }
+            if (etab) {
+                // the units' E tables, precomputed per primitive pair: a coalesced copy
+                const int ne3 = 3 * g.nea;
+                for (int e = tid; e < nb * ne3; e += kGenThreads) {
+                    const int ub = e / ne3, r = e - ub * ne3;
+                    const int pp = pb + (u0 + ub) / nkp;
+                    sUnit[ub * g.unit_dbl + unit_e(g) + r] = __ldg(etab + (size_t)pp * ne3 + r);
                 }
             }
             __syncthreads();
@@ -654,6 +669,32 @@ int general_chunks(int li, int lj, int lk, bool point, bool spherical) {
     return general_shape(li, lj, lk, point, spherical).n_chunks;
 }
 
+// E tables of a pair class for the general kernel: one thread per shell pair,
+// 3 (x, y, z) x (l_i+1)(l_j+1)(l_i+l_j+1) doubles per primitive pair.
+__global__ void general_e_table_kernel(int li, int lj, BraTable bra, double* __restrict__ out) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= bra.n_group) return;
+    const int nea = (li + 1) * (lj + 1) * (li + lj + 1);
+    const double4 AB = bra.grp_AB[g];
+    for (int pp = bra.grp_begin[g]; pp < bra.grp_begin[g + 1]; pp++) {
+        const double4 PA = bra.prim_PA[pp];
+        const double inv2p = 0.5 / bra.prim_P[pp].w;
+        double* E = out + (size_t)pp * 3 * nea;
+        general_e_axis(li, lj, PA.x, AB.x, inv2p, E);
+        general_e_axis(li, lj, PA.y, AB.y, inv2p, E + nea);
+        general_e_axis(li, lj, PA.z, AB.z, inv2p, E + 2 * nea);
+    }
+}
+
+int general_e_doubles(int li, int lj) { return 3 * (li + 1) * (lj + 1) * (li + lj + 1); }
+
+int launch_general_e_table(int li, int lj, const BraTable& bra, double* out, cudaStream_t s) {
+    if (li < 0 || li > lj || li + lj > 2 * kMaxOrbitalL) return 1;
+    if (bra.n_group == 0) return 0;
+    general_e_table_kernel<<<(bra.n_group + 127) / 128, 128, 0, s>>>(li, lj, bra, out);
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
 int general_block_entries(int li, int lj, int lk, bool point, bool spherical) {
     const GenShape g = general_shape(li, lj, lk, point, spherical);
     return g.nij * g.ko_chunk;
@@ -691,6 +732,7 @@ int launch_general_multi(const GenClassSpec* specs, int n, bool spherical, const
             return 3;
         d.g.n_splits = sp.n_splits;
         d.partial = sp.partial;
+        d.etab = sp.etab;
         d.arrive = sp.arrive;
         lp.item0[c] = (int)total;
         total += sp.n_items;
