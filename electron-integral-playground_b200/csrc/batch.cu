@@ -149,6 +149,7 @@ struct eip_batch {
     double* d_split = nullptr;         // partial blocks of the split general classes
     double* d_gen_etab = nullptr;      // E tables of the pair classes that general classes use
     std::map<std::pair<int, int>, size_t> gen_etab_offset;
+    std::map<std::pair<int, int>, int> gen_etab_nprim;  // primitive pairs of those pair classes
     int* d_arrive = nullptr;           // their arrival counters (0 between launches)
     std::vector<size_t> gen_perm_off;  // per group, int2 offset into the orders (or SIZE_MAX)
     // density-fitting plan (eip_batch_df_plan): block list on the device
@@ -713,6 +714,7 @@ int eip_batch_build(eip_batch* b) {
             const std::pair<int, int> pc{pl.li, pl.lj};
             if (b->gen_etab_offset.count(pc)) continue;
             b->gen_etab_offset[pc] = gen_etab_doubles;
+            b->gen_etab_nprim[pc] = (int)bh[pc].P.size();
             gen_etab_doubles += (size_t)general_e_doubles(pl.li, pl.lj) * bh[pc].P.size();
         }
         if (gen_etab_doubles > 0) {
@@ -764,7 +766,7 @@ static int launch_gen_etabs(eip_batch* b, cudaStream_t s, unsigned long long* la
     int rc = 0;
     for (const auto& kv : b->gen_etab_offset) {
         rc |= launch_general_e_table(kv.first.first, kv.first.second, b->bra_by_class[kv.first],
-                                     b->d_gen_etab + kv.second, s);
+                                     b->gen_etab_nprim[kv.first], b->d_gen_etab + kv.second, s);
         if (launches) ++*launches;
     }
     return rc;
@@ -955,7 +957,8 @@ int eip_batch_run_class(eip_batch* b, int i_L, int j_L, int k_L) {
         if (!pl.fast) {
             auto et = b->gen_etab_offset.find({pl.li, pl.lj});
             if (et != b->gen_etab_offset.end())
-                rc |= launch_general_e_table(pl.li, pl.lj, pl.bra, b->d_gen_etab + et->second, b->stream);
+                rc |= launch_general_e_table(pl.li, pl.lj, pl.bra, b->gen_etab_nprim[{pl.li, pl.lj}],
+                                             b->d_gen_etab + et->second, b->stream);
             const GenClassSpec sp = gen_spec(b, pl, pl.map, pl.total_items, b->stream);
             rc |= launch_general_multi(&sp, 1, b->spherical, nullptr, b->omega, b->d_out, pl.counter, b->stream);
         }

@@ -59,7 +59,7 @@ double general_item_cost(int li, int lj, int lk, bool point, bool spherical);
 // E tables of pair class (li, lj) for the general kernel (GenClassSpec::etab):
 // general_e_doubles(li, lj) doubles per primitive pair of the bra table.
 int general_e_doubles(int li, int lj);
-int launch_general_e_table(int li, int lj, const BraTable& bra, double* out, cudaStream_t s);
+int launch_general_e_table(int li, int lj, const BraTable& bra, int n_prim, double* out, cudaStream_t s);
 // Entries of one item's Cartesian accumulator block (the partial block that a
 // split item writes).
 int general_block_entries(int li, int lj, int lk, bool point, bool spherical);

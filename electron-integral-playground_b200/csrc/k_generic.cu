@@ -15,10 +15,15 @@
 // c_library/mcmurchie_davidson_E_term.hpp:22-45, 166-199).  Per block of
 // kGenUB units (primitive pair x auxiliary primitive) the CTA first evaluates,
 // one thread per unit, the prefactor, Boys function, scaled R^{(m)}_000 and
-// coordinate powers, and per unit and axis the E^{ij}_t table; then, unit by
-// unit, all threads split (1) the Hermite tetrahedron R_{tuv} (closed form),
-// (2) the ket contraction X[h][k], (3) the bra contraction into accumulators
-// held in registers (kGenAcc per thread).  (Transferring after the
+// coordinate powers, and per unit and axis the E^{ij}_t table (or, in a
+// batch, copies it from the table precomputed per primitive pair by
+// general_e_table_kernel); then, unit by unit, all threads split (1) the
+// Hermite tetrahedron R_{tuv} (closed form), (2) the ket contraction X[h][k]
+// (stored v-innermost, spherical kets through compact lists of their non-zero
+// terms), (3) the bra contraction into accumulators held in registers
+// (kGenAcc per thread; the bra pairs ranked by their loop shape so that a
+// warp's lanes run the same trip counts).  Blocks with many units are split
+// into several items whose partial blocks the last to arrive adds up.  (Transferring after the
 // contraction instead, as the fast FP64 kernels do for l <= 2, loses up to
 // 1e-9 to cancellation for g-g pairs with distant centres and extreme
 // exponents, so the high-l classes transfer per primitive pair.)
@@ -669,29 +674,34 @@ int general_chunks(int li, int lj, int lk, bool point, bool spherical) {
     return general_shape(li, lj, lk, point, spherical).n_chunks;
 }
 
-// E tables of a pair class for the general kernel: one thread per shell pair,
-// 3 (x, y, z) x (l_i+1)(l_j+1)(l_i+l_j+1) doubles per primitive pair.
-__global__ void general_e_table_kernel(int li, int lj, BraTable bra, double* __restrict__ out) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= bra.n_group) return;
-    const int nea = (li + 1) * (lj + 1) * (li + lj + 1);
-    const double4 AB = bra.grp_AB[g];
-    for (int pp = bra.grp_begin[g]; pp < bra.grp_begin[g + 1]; pp++) {
-        const double4 PA = bra.prim_PA[pp];
-        const double inv2p = 0.5 / bra.prim_P[pp].w;
-        double* E = out + (size_t)pp * 3 * nea;
-        general_e_axis(li, lj, PA.x, AB.x, inv2p, E);
-        general_e_axis(li, lj, PA.y, AB.y, inv2p, E + nea);
-        general_e_axis(li, lj, PA.z, AB.z, inv2p, E + 2 * nea);
+// E tables of a pair class for the general kernel: one thread per (primitive
+// pair, axis), 3 (x, y, z) x (l_i+1)(l_j+1)(l_i+l_j+1) doubles per primitive pair.
+__global__ void general_e_table_kernel(int li, int lj, BraTable bra, int n_prim, double* __restrict__ out) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= 3 * n_prim) return;
+    const int pp = w / 3, d = w - 3 * pp;
+    // the primitive pair's shell pair: last g with grp_begin[g] <= pp
+    int lo = 0, hi = bra.n_group - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(bra.grp_begin + mid) <= pp) lo = mid;
+        else hi = mid - 1;
     }
+    const int nea = (li + 1) * (lj + 1) * (li + lj + 1);
+    const double4 AB = bra.grp_AB[lo];
+    const double4 PA = bra.prim_PA[pp];
+    const double pa_d = d == 0 ? PA.x : (d == 1 ? PA.y : PA.z);
+    const double ab_d = d == 0 ? AB.x : (d == 1 ? AB.y : AB.z);
+    general_e_axis(li, lj, pa_d, ab_d, 0.5 / bra.prim_P[pp].w, out + ((size_t)pp * 3 + d) * nea);
 }
 
 int general_e_doubles(int li, int lj) { return 3 * (li + 1) * (lj + 1) * (li + lj + 1); }
 
-int launch_general_e_table(int li, int lj, const BraTable& bra, double* out, cudaStream_t s) {
+int launch_general_e_table(int li, int lj, const BraTable& bra, int n_prim, double* out, cudaStream_t s) {
     if (li < 0 || li > lj || li + lj > 2 * kMaxOrbitalL) return 1;
-    if (bra.n_group == 0) return 0;
-    general_e_table_kernel<<<(bra.n_group + 127) / 128, 128, 0, s>>>(li, lj, bra, out);
+    if (bra.n_group == 0 || n_prim <= 0) return 0;
+    if (n_prim > 0x7fffffff / 3) return 3;
+    general_e_table_kernel<<<(3 * n_prim + 127) / 128, 128, 0, s>>>(li, lj, bra, n_prim, out);
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
