@@ -54,10 +54,12 @@ namespace eip {
 //   ACC   accumulators (doubles) per lane -> how many warps split the ket
 //   WARPS resident warps per SM asked of the register allocator (register cap
 //         65536 / (32 * WARPS)); more warps hide latency, fewer avoid spills.
-//   v0 48/16, v1 48/8, v2 24/16, v3 96/8, v4 24/24, v5 48/24
+//   v0 48/16, v1 32/16, v2 24/16, v3 96/8, v4 24/24, v5 48/24
 constexpr int kVariants = 6;
-__host__ __device__ constexpr int variant_acc(int v) { return v == 2 || v == 4 ? 24 : (v == 3 ? 96 : 48); }
-__host__ __device__ constexpr int variant_warps(int v) { return v == 1 || v == 3 ? 8 : (v >= 4 ? 24 : 16); }
+__host__ __device__ constexpr int variant_acc(int v) {
+    return v == 2 || v == 4 ? 24 : (v == 3 ? 96 : (v == 1 ? 32 : 48));
+}
+__host__ __device__ constexpr int variant_warps(int v) { return v == 3 ? 8 : (v >= 4 ? 24 : 16); }
 
 // E table record of one primitive pair (e_table_kernel): for l_i > 0, l_j >= 2 first
 // E^{0 b}_t, b <= l_i + l_j, for x, y, z (the transfer-after-contraction
@@ -721,41 +723,50 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                 } else {
                     // Several warps: the same code in every warp, coefficients
                     // from constant memory, so the instruction cache holds one copy.
-                    T Xh[C::KPW][C::NHB];
+                    // A warp owning several components forms X for all of them at
+                    // once (one tetrahedron load feeds each), or, when that block
+                    // would exceed kXMaxMW values, one component at a time.
+                    constexpr int kXMaxMW = 24;
+                    constexpr int XC = C::KPW * C::NHB > kXMaxMW ? 1 : C::KPW;  // components per X block
+                    static_for<0, C::KPW / XC>([&](auto q_) {
+                        constexpr int c0 = decltype(q_)::value * XC;
+                        if constexpr (c0 > 0) asm volatile("" ::: "memory");
+                        T Xh[XC][C::NHB];
 #pragma unroll
-                    for (int c = 0; c < C::KPW; c++)
+                        for (int c = 0; c < XC; c++)
 #pragma unroll
-                        for (int h = 0; h < C::NHB; h++) Xh[c][h] = T(0);
-                    int sidx = 0;
-                    // top Hermite level |s| = LK only (ket_top_level_only)
-                    static_for<0, 1>([&](auto j_) {
-                        constexpr int j = decltype(j_)::value;
-                        constexpr int S = LK - 2 * j;
-                        static_for<0, ncart(S)>([&](auto sc_) {
-                            constexpr int sc = decltype(sc_)::value;
-                            constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
-                            T ce[C::KPW];
-                            bool any = false;
+                            for (int h = 0; h < C::NHB; h++) Xh[c][h] = T(0);
+                        int sidx = 0;
+                        // top Hermite level |s| = LK only (ket_top_level_only)
+                        static_for<0, 1>([&](auto j_) {
+                            constexpr int j = decltype(j_)::value;
+                            constexpr int S = LK - 2 * j;
+                            static_for<0, ncart(S)>([&](auto sc_) {
+                                constexpr int sc = decltype(sc_)::value;
+                                constexpr int sx = cart_x(S, sc), sy = cart_y(S, sc), sz = cart_z(S, sc);
+                                T ce[XC];
+                                bool any = false;
 #pragma unroll
-                            for (int c = 0; c < C::KPW; c++) {
-                                const int ko = warp * C::KPW + c;
-                                const double cf = ko < C::NKO ? c_ket_coef<LK>.v[ko][sidx + sc] : 0.0;
-                                ce[c] = (T)cf * w[j];
-                                any = any || cf != 0.0;
-                            }
-                            if (any) {  // warp-uniform
-                                static_for<0, C::NHB>([&](auto h_) {
-                                    constexpr int h = decltype(h_)::value;
-                                    constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
-                                    const T r = sR[(herm_index(t + sx, u + sy, v + sz) - C::R0) * 32 + lane];
+                                for (int c = 0; c < XC; c++) {
+                                    const int ko = warp * C::KPW + c0 + c;
+                                    const double cf = ko < C::NKO ? c_ket_coef<LK>.v[ko][sidx + sc] : 0.0;
+                                    ce[c] = (T)cf * w[j];
+                                    any = any || cf != 0.0;
+                                }
+                                if (any) {  // warp-uniform
+                                    static_for<0, C::NHB>([&](auto h_) {
+                                        constexpr int h = decltype(h_)::value;
+                                        constexpr int t = herm_t(h), u = herm_u(h), v = herm_v(h);
+                                        const T r = sR[(herm_index(t + sx, u + sy, v + sz) - C::R0) * 32 + lane];
 #pragma unroll
-                                    for (int c = 0; c < C::KPW; c++) Xh[c][h] = fma(ce[c], r, Xh[c][h]);
-                                });
-                            }
+                                        for (int c = 0; c < XC; c++) Xh[c][h] = fma(ce[c], r, Xh[c][h]);
+                                    });
+                                }
+                            });
+                            sidx += ncart(S);
                         });
-                        sidx += ncart(S);
+                        bra_acc(Xh, ic<c0>{}, ic<XC>{});
                     });
-                    bra_acc(Xh, ic<0>{}, ic<C::KPW>{});
                 }
                 if constexpr (ONE) __syncwarp();
                 else __syncthreads();
