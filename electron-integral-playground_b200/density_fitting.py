@@ -203,7 +203,11 @@ class BatchCoulomb:
         self.stream = torch.cuda.ExternalStream(batch.stream)
 
     def fit(self, D):
-        """gamma = (mu nu|P) D for every molecule (D: concatenated densities)."""
+        """gamma = (mu nu|P) D for every molecule (D: concatenated densities).
+        The batch stream first waits for the current torch stream, where D and
+        this object's buffers and (inverted) factors were made; solve and
+        coulomb follow on the batch stream."""
+        self.stream.wait_stream(self.torch.cuda.current_stream())
         self.batch.df_gamma(D.data_ptr(), self.gamma.data_ptr())
 
     def solve(self):
@@ -225,10 +229,7 @@ class BatchCoulomb:
 
     def run(self, D):
         """D: concatenated densities (device tensor of n_ao2 doubles).  Returns
-        the concatenated J (device tensor; valid once the batch stream is done).
-        The batch stream first waits for the current torch stream, where D and
-        this object's buffers and (inverted) factors were made."""
-        self.stream.wait_stream(self.torch.cuda.current_stream())
+        the concatenated J (device tensor; valid once the batch stream is done)."""
         self.fit(D)
         self.solve()
         self.coulomb()
