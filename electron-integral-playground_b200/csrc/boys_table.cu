@@ -9,7 +9,9 @@
 
 namespace eip {
 
-__device__ double g_boys_table[kBoysGrid * kBoysOrders];
+// order-major: row (L, i) = F_L..F_{L+kBoysTaylor-1}(T0_i), 64-byte aligned (boys_row)
+constexpr size_t kBoysTableDoubles = (size_t)(kMaxBoysM + 1) * kBoysGrid * kBoysTaylor;
+__device__ __align__(64) double g_boys_table[kBoysTableDoubles];
 
 namespace {
 // Device address of g_boys_table per device (nullptr: tables not uploaded yet).
@@ -34,7 +36,9 @@ static void build_boys_table(double* out) {
         }
         F[M] = eT * sum;
         for (int m = M - 1; m >= 0; m--) F[m] = (2.0L * T * F[m + 1] + eT) / (2 * m + 1);
-        for (int m = 0; m <= M; m++) out[i * kBoysOrders + m] = (double)F[m];
+        for (int L = 0; L <= kMaxBoysM; L++)
+            for (int k = 0; k < kBoysTaylor; k++)
+                out[((size_t)L * kBoysGrid + i) * kBoysTaylor + k] = (double)F[L + k];
     }
 }
 
@@ -44,7 +48,7 @@ int ensure_device_tables() {
     if (g_boys_address[dev].load(std::memory_order_acquire)) return 0;
     std::lock_guard<std::mutex> lock(g_tables_mu);
     if (g_boys_address[dev].load(std::memory_order_acquire)) return 0;
-    static double host_table[kBoysGrid * kBoysOrders];
+    static double host_table[kBoysTableDoubles];
     static bool built = false;
     if (!built) {
         build_boys_table(host_table);

@@ -163,8 +163,22 @@ __device__ __forceinline__ void static_for(F&& f) {
 //            stable downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1).
 //   T >= 36: F_0 = sqrt(pi/T)/2 (erf(sqrt T) = 1 in FP64) and the upward
 //            recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T), stable for m < T.
-// `table` is the device address of the grid (kBoysGrid x kBoysOrders doubles),
-// passed to every kernel as an argument.
+// `table` is the device address of the grid ((kMaxBoysM + 1) x kBoysGrid x
+// kBoysTaylor doubles, order-major, see boys_row), passed to every kernel as
+// an argument.
+// The grid is stored order-major: for each order L and grid point i the
+// kBoysTaylor values F_L..F_{L+7}(T0_i) are one aligned 64-byte row
+// (table + (L kBoysGrid + i) kBoysTaylor), read with four 16-byte loads.
+__device__ __forceinline__ void boys_row(const double* __restrict__ table, int L, int i, double* c) {
+    const double2* r = reinterpret_cast<const double2*>(table + ((size_t)L * kBoysGrid + i) * kBoysTaylor);
+#pragma unroll
+    for (int k = 0; k < kBoysTaylor / 2; k++) {
+        const double2 v = __ldg(r + k);
+        c[2 * k] = v.x;
+        c[2 * k + 1] = v.y;
+    }
+}
+
 template <int L>
 __device__ __forceinline__ void boys(const double* __restrict__ table, double T, double* F) {
     static_assert(L >= 0 && L <= kMaxBoysM, "Boys order out of range");
@@ -172,10 +186,11 @@ __device__ __forceinline__ void boys(const double* __restrict__ table, double T,
     if (T < kBoysTMax) {
         const int i = __double2int_rn(T * kBoysInvStep);
         const double d = T - i * kBoysStep;
-        const double* row = table + i * kBoysOrders + L;
-        double acc = __ldg(row + kBoysTaylor - 1);
+        double c[kBoysTaylor];
+        boys_row(table, L, i, c);
+        double acc = c[kBoysTaylor - 1];
 #pragma unroll
-        for (int k = kBoysTaylor - 1; k >= 1; k--) acc = fma(-d * (1.0 / k), acc, __ldg(row + k - 1));
+        for (int k = kBoysTaylor - 1; k >= 1; k--) acc = fma(-d * (1.0 / k), acc, c[k - 1]);
         F[L] = acc;
         const double twoT = 2.0 * T;
 #pragma unroll
@@ -205,9 +220,11 @@ __device__ __forceinline__ void boys_rt(const double* __restrict__ table, int L,
     if (T < kBoysTMax) {
         const int i = __double2int_rn(T * kBoysInvStep);
         const double d = T - i * kBoysStep;
-        const double* row = table + i * kBoysOrders + L;
-        double acc = __ldg(row + kBoysTaylor - 1);
-        for (int k = kBoysTaylor - 1; k >= 1; k--) acc = fma(-d * c_inv_n[k], acc, __ldg(row + k - 1));
+        double c[kBoysTaylor];
+        boys_row(table, L, i, c);
+        double acc = c[kBoysTaylor - 1];
+#pragma unroll
+        for (int k = kBoysTaylor - 1; k >= 1; k--) acc = fma(-d * c_inv_n[k], acc, c[k - 1]);
         F[L] = acc;
         for (int m = L - 1; m >= 0; m--) F[m] = fma(2.0 * T, F[m + 1], eT) * c_inv_n[2 * m + 1];
     } else {
