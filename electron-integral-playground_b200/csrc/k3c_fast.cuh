@@ -54,12 +54,14 @@ namespace eip {
 //   ACC   accumulators (doubles) per lane -> how many warps split the ket
 //   WARPS resident warps per SM asked of the register allocator (register cap
 //         65536 / (32 * WARPS)); more warps hide latency, fewer avoid spills.
-//   v0 48/16, v1 32/16, v2 24/16, v3 96/8, v4 24/24, v5 48/24
+//   XMAX  one-warp CTAs: the ket contraction X of at most this many values per
+//         lane at a time (more components go in chunks: fewer live registers,
+//         the tetrahedron read once per chunk)
+//   v0 48/16, v1 48/16 with X chunks of 24, v2 24/16, v3 96/8, v4 24/24, v5 48/24
 constexpr int kVariants = 6;
-__host__ __device__ constexpr int variant_acc(int v) {
-    return v == 2 || v == 4 ? 24 : (v == 3 ? 96 : (v == 1 ? 32 : 48));
-}
+__host__ __device__ constexpr int variant_acc(int v) { return v == 2 || v == 4 ? 24 : (v == 3 ? 96 : 48); }
 __host__ __device__ constexpr int variant_warps(int v) { return v == 3 ? 8 : (v >= 4 ? 24 : 16); }
+__host__ __device__ constexpr int variant_xmax(int v) { return v == 1 ? 24 : 48; }
 
 // E table record of one primitive pair (e_table_kernel): for l_i > 0, l_j >= 2 first
 // E^{0 b}_t, b <= l_i + l_j, for x, y, z (the transfer-after-contraction
@@ -670,7 +672,7 @@ k3c_fast(const double* __restrict__ boys_table, BraTable bra, KetTable ket, Batc
                     // constants (zero terms vanish).  When X[KPW][NHB] would hold
                     // more than kXMax values, the components go in chunks (fewer
                     // live registers; an R entry is loaded once per chunk).
-                    constexpr int kXMax = 48;
+                    constexpr int kXMax = variant_xmax(V);
                     constexpr int NCH = (C::KPW * C::NHB + kXMax - 1) / kXMax;
                     constexpr int KCH = (C::KPW + NCH - 1) / NCH;
                     static_for<0, (C::KPW + KCH - 1) / KCH>([&](auto q_) {
