@@ -964,12 +964,12 @@ def main():
         [tot["screened"], tot["primitive"], tot["contracted"], sum(len(m.elements) for m in mols), out_bytes / 8],
         torch.distributed.ReduceOp.SUM if world > 1 else None, "cuda")
     value = screened / (head["ms"] * 1e-3)
-    # copy bandwidth measured on this pool's B200s; without the measured file,
-    # the earlier pool measurement of 6.65 TB/s ("of fallback")
-    hbm_peak, hbm_source = 6650.0, "fallback 6.65 TB/s (earlier copy-bandwidth measurement on this pool)"
+    # measured copy bandwidth of the B200s (MEASURED_PEAKS.json); without that
+    # file, an earlier copy-bandwidth measurement of 6.65 TB/s ("of fallback")
+    hbm_peak, hbm_source = 6650.0, "fallback 6.65 TB/s (earlier copy-bandwidth measurement on B200)"
     try:
         hbm_peak = float(json.loads((REPO / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
-        hbm_source = "MEASURED_PEAKS.json hbm_gbs (copy bandwidth measured on this pool)"
+        hbm_source = "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth of this GPU model)"
     except Exception:
         pass
     roof = None

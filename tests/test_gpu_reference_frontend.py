@@ -7,7 +7,7 @@ LD_LIBRARY_PATH, set no argtypes or restype, pass every scalar wrapped in
 ctypes.c_int / c_bool / c_double and every array as ``ndarray.ctypes.data_as``
 a double or int pointer, and assert a return value of 0 per class call
 (three_center.py:28-48).  The wrappers themselves are not shipped here (they
-are the reference's source and do not exist on the GPU box), so this test
+are the reference's source, absent where the GPU tests run), so this test
 makes the same calls in the same form from a child process whose
 LD_LIBRARY_PATH holds only this library's directory, checks that the library
 it loaded by that bare name is this one, and compares the four integrals of
