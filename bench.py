@@ -309,7 +309,7 @@ def run_serving(args, torch, seed):
     }
 
 
-def run_config2(torch, bt, threshold, seed=0, window_bytes=24e9):
+def run_water100_windows(torch, bt, threshold, seed=0, window_bytes=24e9):
     """100-water cluster (300 atoms, 15 A cube, aux s-f): every (mu nu|P) in
     FP64 and in mixed precision, window by window over the auxiliary basis on
     resident tables; max abs / rel error of mixed vs FP64 per class, triplets/s
@@ -426,7 +426,7 @@ def aux_slice(aux_data, n_aux, frac):
     return out
 
 
-def run_config0(seed=0):
+def run_water10_per_type(seed=0):
     """10-water cluster (30 atoms), O 3s2p1d / H 2s1p, aux s-f, spherical: S, V,
     (P|Q) and (mu nu|P) through the drop-in C ABI (host arrays in and out, the
     reference front end's per-class calls), each timed as best of 3 after a
@@ -498,7 +498,7 @@ def run_config0(seed=0):
     return out
 
 
-def run_config3(torch, bt, fp64_peak, steps=5, seed=0, reference=True):
+def run_random_high_l_triplets(torch, bt, fp64_peak, steps=5, seed=0, reference=True):
     """2000 random shell triplets (orbital l <= 4, aux l <= 5, 1-8 primitives,
     exponents log-uniform in [0.05, 1e4], centres in a 6 A cube), each its own
     molecule slot of one batch: FP64 and mixed precision, one CUDA-graph launch
@@ -702,14 +702,14 @@ def main():
     ap.add_argument("--serve-alone", type=int, default=40, help="requests also timed alone in FP64")
     ap.add_argument("--no-e2e-df", dest="e2e_df", action="store_false",
                     help="e2e returns per-molecule checksums instead of the density-fitted J (profiling runs)")
-    ap.add_argument("--no-config0", action="store_true", help="skip the 10-water per-type timings")
-    ap.add_argument("--no-config3", action="store_true", help="skip the 2000 high-l random triplets")
-    ap.add_argument("--only-config3", action="store_true",
+    ap.add_argument("--no-water10", action="store_true", help="skip the 10-water per-type timings")
+    ap.add_argument("--no-high-l", action="store_true", help="skip the 2000 high-l random triplets")
+    ap.add_argument("--only-high-l", action="store_true",
                     help="time only the 2000 high-l random triplets (FP64 and mixed; the line's value is FP64 "
                          "triplets/s); for profiling the general kernel")
     ap.add_argument("--no-mixed-reference", action="store_true",
                     help="skip the mixed-precision error against the reference library")
-    ap.add_argument("--no-config2", action="store_true",
+    ap.add_argument("--no-water100", action="store_true",
                     help="skip the 100-water mixed-vs-FP64 per-class measurement")
     ap.add_argument("--tune", action="store_true",
                     help="run the autotuner on this workload first and rewrite its cache")
@@ -739,8 +739,8 @@ def main():
     if lm.lib().eip_init(local) != 0:
         raise RuntimeError(lm.lib().eip_last_error().decode())
 
-    if args.only_config3:
-        c3 = run_config3(torch, bt, bt.measure_fma_peak(), steps=args.steps, seed=args.seed, reference=False)
+    if args.only_high_l:
+        c3 = run_random_high_l_triplets(torch, bt, bt.measure_fma_peak(), steps=args.steps, seed=args.seed, reference=False)
         if rank == 0:
             print(json.dumps({"metric": "random high-l shell triplets/s (FP64)", "value": c3["fp64"]["triplets_per_s"],
                               "unit": "triplets/s", "n_gpus": 1, "steps": args.steps, "warmup": 3,
@@ -1014,16 +1014,16 @@ def main():
                              f"{smp['triplets']} screened triplets, {smp['seconds']:.1f} s, all host threads",
                    "gpu_same_sample": same_sample_rate(bt, torch, mols, pds, ads, smp, args)}
             dropin = dropin_sample(mols, pds, ads, stats, smp["molecules"])
-    config0 = config3 = mixed_ref = None
+    water10 = high_l = mixed_ref = None
     if rank == 0 and world == 1:
-        if not args.no_config0:
-            config0 = run_config0(args.seed)
-        if not args.no_config3:
-            config3 = run_config3(torch, bt, fp64_peak, seed=args.seed)
+        if not args.no_water10:
+            water10 = run_water10_per_type(args.seed)
+        if not args.no_high_l:
+            high_l = run_random_high_l_triplets(torch, bt, fp64_peak, seed=args.seed)
         if not args.no_mixed_reference:
             mixed_ref = run_mixed_vs_reference(bt, mols, pds, ads, args.fp32_threshold)
     serving = run_serving(args, torch, args.seed) if args.serve_requests > 0 and rank == 0 else None
-    config2 = run_config2(torch, bt, args.fp32_threshold, args.seed) if not args.no_config2 and rank == 0 else None
+    water100 = run_water100_windows(torch, bt, args.fp32_threshold, args.seed) if not args.no_water100 and rank == 0 else None
     if rank == 0:
         per = head["per_step"]
         line = {
@@ -1074,7 +1074,7 @@ def main():
                         "coulomb_gbs": out_bytes / (head["df_coulomb_ms"] * 1e-3) / 1e9,
                         "solve": head.get("df_solve")}},
             "roofline": roof, "cpu_baseline": cpu, "dropin_fp64": dropin, "serving": serving,
-            "water100_mixed_vs_fp64": config2, "water10_per_type": config0, "random_triplets_high_l": config3,
+            "water100_mixed_vs_fp64": water100, "water10_per_type": water10, "random_triplets_high_l": high_l,
             "mixed_vs_reference": mixed_ref,
             "gpu_launches": head["launches"], "clocks": head["clocks"], "clocks_fp64": m64["clocks"],
             "latency_ms": {"p50": statistics.median(per), "p99": sorted(per)[min(len(per) - 1, int(0.99 * len(per)))],

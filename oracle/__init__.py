@@ -1,4 +1,4 @@
-"""CPU checkers for the integral path -- TEST INFRASTRUCTURE ONLY.
+"""CPU references for the integral path -- TEST INFRASTRUCTURE ONLY.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may
 import this package, and only to check or time against it; the product path

@@ -1,7 +1,7 @@
 /*
  * CPU oracle for the McMurchie-Davidson integral path -- TEST INFRASTRUCTURE.
  * Used only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
- * as the checker; never linked into, or called by, the product library.
+ * as the reference to verify against; never linked into, or called by, the product library.
  *
  * Restatement of the reference drivers, primitive triplet by primitive
  * triplet, in plain C with runtime angular momenta:

@@ -2,8 +2,8 @@
  * CPU oracle for the McMurchie-Davidson integral path -- TEST INFRASTRUCTURE.
  *
  * A plain-C restatement of the reference's four integral drivers, used only
- * by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the
- * checker.  Never linked into the product library.
+ * by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg, to
+ * verify results against.  Never linked into the product library.
  *
  * Entry points take exactly the arguments of the reference C ABI
  * (electron_integral_playground/c_library/molecular_integral/*.cpp) and have

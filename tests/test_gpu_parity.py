@@ -1,7 +1,7 @@
 """GPU parity of the drop-in C ABI against the reference.
 
 Every call goes through libmolecular_integral.so's reference-compatible entry
-points (via the package's ctypes front end).  Checkers:
+points (via the package's ctypes front end).  References:
 * the reference library itself, compiled from its sources into oracle/_ref/
   (run on the same inputs, on the host cores), at 1e-12 absolute -- the bar
   for the plain FP64 path;
@@ -116,7 +116,7 @@ def test_device_boys_against_series():
 
 
 def test_random_high_angular_triplets():
-    """Config-3-like random shell triplets (orbital l <= 4, aux l <= 5,
+    """Random high-angular-momentum shell triplets (orbital l <= 4, aux l <= 5,
     1-8 primitives, exponents log-uniform in [0.05, 1e4]) against the oracle."""
     ds = importlib.import_module("electron-integral-playground_b200.data_structure")
     rng = np.random.default_rng(3)
