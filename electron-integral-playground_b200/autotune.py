@@ -17,7 +17,7 @@ import pathlib
 
 from ._lib import lib
 
-N_VARIANTS = 6
+N_VARIANTS = 7
 FP32_VARIANTS = (0, 2, 3, 4)
 DEFAULT_CACHE = pathlib.Path(__file__).resolve().parent / "tuning" / "b200_fp64.json"
 

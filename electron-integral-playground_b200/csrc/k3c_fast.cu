@@ -17,7 +17,7 @@ namespace eip {
                                         double* out, int* counter, cudaStream_t s);
 #define EIP_DECL(I, J)                                                                                      \
     EIP_DECL_V(I, J, 0) EIP_DECL_V(I, J, 1) EIP_DECL_V(I, J, 2) EIP_DECL_V(I, J, 3) EIP_DECL_V(I, J, 4)     \
-    EIP_DECL_V(I, J, 5)                                                                                     \
+    EIP_DECL_V(I, J, 5) EIP_DECL_V(I, J, 6)                                                                 \
     EIP_DECL_F(I, J, 0) EIP_DECL_F(I, J, 2) EIP_DECL_F(I, J, 3) EIP_DECL_F(I, J, 4)                          \
     int launch_e_table_##I##J(const BraTable& bra, double* prim_E, cudaStream_t s);
 EIP_DECL(0, 0) EIP_DECL(0, 1) EIP_DECL(1, 1) EIP_DECL(0, 2) EIP_DECL(1, 2) EIP_DECL(2, 2) EIP_DECL(0, 3) EIP_DECL(0, 4)
@@ -30,6 +30,7 @@ EIP_DECL(0, 0) EIP_DECL(0, 1) EIP_DECL(1, 1) EIP_DECL(0, 2) EIP_DECL(1, 2) EIP_D
 // A = B = P).  Variant per (l_i, l_j, l_k), default 0; the autotuner's choices
 // on B200 (tuning/b200_fp64.json) are applied with eip_tune_set.
 static int g_variant[5][5][5] = {};
+constexpr int kVariantsHost = 7;  // FP64 launch variants compiled (k3c_fast.cuh: kVariants)
 // FP32 (mixed-precision) kernels: compiled variants 0, 2, 3, 4; default 0.
 static int g_variant32[5][5][5] = {};
 
@@ -43,7 +44,7 @@ int fast3c_variant(int li, int lj, int lk) {
 }
 
 int fast3c_set_variant(int li, int lj, int lk, int v) {
-    if (!fast3c_supported(li, lj, lk) || v < 0 || v > 5) return 1;
+    if (!fast3c_supported(li, lj, lk) || v < 0 || v >= kVariantsHost) return 1;
     g_variant[li][lj][lk] = v;
     return 0;
 }
@@ -82,6 +83,7 @@ int launch_fast3c(int li, int lj, int lk, const BraTable& bra, const KetTable& k
         case 3: EIP_GO_V(I, J, 3);                                                                            \
         case 4: EIP_GO_V(I, J, 4);                                                                            \
         case 5: EIP_GO_V(I, J, 5);                                                                            \
+        case 6: EIP_GO_V(I, J, 6);                                                                            \
         case -1: return launch_fast3c_##I##J##_f32_v0(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
         case -3: return launch_fast3c_##I##J##_f32_v2(lk, t, bra, ket, map, total_items, omega, out, counter, s); \
         case -4: return launch_fast3c_##I##J##_f32_v3(lk, t, bra, ket, map, total_items, omega, out, counter, s); \

@@ -15,6 +15,7 @@ syn = importlib.import_module("electron-integral-playground_b200.synthetic")
 pu = importlib.import_module("electron-integral-playground_b200.pair_utility")
 mi = importlib.import_module("electron-integral-playground_b200.molecular_integral")
 bt = importlib.import_module("electron-integral-playground_b200.batch")
+at = importlib.import_module("electron-integral-playground_b200.autotune")
 
 
 @pytest.fixture(scope="module")
@@ -84,7 +85,7 @@ def test_every_tuning_variant_matches_reference(small_batch):
     want = oracle.drive_three_center(ref, pds[3], ads[3], mols[3])
     saved = {(li, lj, lk): L.eip_tune_get(li, lj, lk) for (li, lj) in pds[3] for lk in ads[3]}
     try:
-        for v in range(6):
+        for v in range(at.N_VARIANTS):
             for (li, lj, lk) in saved:
                 if saved[(li, lj, lk)] >= 0:
                     L.eip_tune_set(li, lj, lk, v)
@@ -138,7 +139,7 @@ def test_contracted_auxiliary_every_variant_and_mixed():
     L = lm.lib()
     saved = {(li, lj, lk): L.eip_tune_get(li, lj, lk) for (li, lj) in pd for lk in ad}
     try:
-        for v in range(6):
+        for v in range(at.N_VARIANTS):
             for (li, lj, lk) in saved:
                 if saved[(li, lj, lk)] >= 0:
                     L.eip_tune_set(li, lj, lk, v)
@@ -150,7 +151,6 @@ def test_contracted_auxiliary_every_variant_and_mixed():
                 L.eip_tune_set(*k, v)
     # every shell pair in FP32 (R, ket, bra), through every FP32 launch variant:
     # a loose bound that still catches any misplaced component or unit
-    at = importlib.import_module("electron-integral-playground_b200.autotune")
     saved32 = {k: L.eip_tune_get_fp32(*k) for k in saved}
     try:
         for v in at.FP32_VARIANTS:
