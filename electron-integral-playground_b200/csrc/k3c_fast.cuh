@@ -57,16 +57,16 @@ namespace eip {
 //   XMAX  one-warp CTAs: the ket contraction X of at most this many values per
 //         lane at a time (more components go in chunks: fewer live registers,
 //         the tetrahedron read once per chunk)
-//   v0 48/16, v1 48/16 with X chunks of 24, v2 24/16, v3 96/8, v4 24/24,
-//   v5 96/12 with X chunks of 24, v6 96/8 with X chunks of 24
+//   v0 48/12 with X chunks of 24, v1 48/16 with X chunks of 24, v2 24/16, v3 96/8,
+//   v4 24/24, v5 96/12 with X chunks of 24, v6 96/8 with X chunks of 24
 constexpr int kVariants = 7;
 __host__ __device__ constexpr int variant_acc(int v) {
     return v == 2 || v == 4 ? 24 : (v == 3 || v == 5 || v == 6 ? 96 : 48);
 }
 __host__ __device__ constexpr int variant_warps(int v) {
-    return v == 3 || v == 6 ? 8 : (v == 5 ? 12 : (v == 4 ? 24 : 16));
+    return v == 3 || v == 6 ? 8 : (v == 0 || v == 5 ? 12 : (v == 4 ? 24 : 16));
 }
-__host__ __device__ constexpr int variant_xmax(int v) { return v == 1 || v == 5 || v == 6 ? 24 : 48; }
+__host__ __device__ constexpr int variant_xmax(int v) { return v == 2 || v == 3 || v == 4 ? 48 : 24; }
 
 // E table record of one primitive pair (e_table_kernel): for l_i > 0, l_j >= 2 first
 // E^{0 b}_t, b <= l_i + l_j, for x, y, z (the transfer-after-contraction
